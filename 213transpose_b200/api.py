@@ -1,0 +1,231 @@
+"""Python mirror of kaihsin/213transpose's C++ interface, on top of the C ABI.
+
+Names, argument order and meaning follow the reference:
+
+  inplace.transpose(data, d1, d2, d3)            include/transpose.h:17-18
+  inplace.c2r.transpose(data, d1, d2, d3)        include/transpose.h:5-9
+  inplace.r2c.transpose(data, d1, d2, d3)        include/transpose.h:11-15
+  inplace.detail.rotate(fn, d3, d2, d1, data)    include/rotate.h:6-7
+  inplace.detail.shuffle_fn(data, d3, d2, d1, fn) include/shuffle.h:5-6
+  inplace.detail.col_shuffle_fn(fn, d3, d2, d1, data) include/col_shuffle.h:8-9
+  inplace.detail.scatter_permute(fn, d3, d2, d1, data) include/permute.h:6-7
+  inplace.detail.c2r.skinny_transpose(data, d1, d2, d3) include/skinny.h:9-10
+  inplace.detail.r2c.skinny_transpose(data, d1, d2, d3) include/skinny.h:84-85
+  functors inplace.detail.c2r.* / inplace.detail.r2c.* with the constructor
+  arguments of include/equations.h and include/skinny.h.
+
+`data` is a contiguous CUDA torch.Tensor (element size from its dtype, work on
+its device's current stream) or a raw device pointer with elem_bytes=...
+Where the reference exits or throws, these raise T213Error.
+"""
+from __future__ import annotations
+
+import ctypes
+from types import SimpleNamespace
+
+from . import _lib
+from ._lib import check, lib, params
+
+_torch = None
+
+
+def _t():
+    global _torch
+    if _torch is None:
+        import torch
+        _torch = torch
+    return _torch
+
+
+def _resolve(data, elem_bytes=None, stream=None):
+    """-> (pointer, element bytes, stream handle)"""
+    if hasattr(data, "data_ptr"):
+        torch = _t()
+        if not data.is_cuda:
+            raise ValueError("tensor must live on a CUDA device (use transpose_host for host tensors)")
+        if not data.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        eb = data.element_size() if elem_bytes is None else int(elem_bytes)
+        if stream is None:
+            stream = torch.cuda.current_stream(data.device).cuda_stream
+        elif hasattr(stream, "cuda_stream"):
+            stream = stream.cuda_stream
+        return ctypes.c_void_p(data.data_ptr()), eb, ctypes.c_void_p(int(stream))
+    if elem_bytes is None:
+        raise ValueError("elem_bytes is required with a raw pointer")
+    if hasattr(stream, "cuda_stream"):
+        stream = stream.cuda_stream
+    return ctypes.c_void_p(int(data)), int(elem_bytes), ctypes.c_void_p(int(stream or 0))
+
+
+class Functor:
+    """An index functor of the decomposition: kind (include/t213.h t213_fn)
+    plus the reference constructor's arguments."""
+
+    kind = 0
+    nparams = 0
+    name = "functor"
+
+    def __init__(self, *args):
+        if len(args) != self.nparams:
+            raise TypeError(f"{self.name} takes {self.nparams} arguments")
+        self.params = tuple(int(a) for a in args)
+
+    def __repr__(self):
+        return f"{self.name}{self.params}"
+
+
+def _fn(kind, nparams, name):
+    return type(name, (Functor,), {"kind": kind, "nparams": nparams, "name": name})
+
+
+# inplace::detail::c2r (include/equations.h, include/skinny.h)
+_c2r_prerotator = _fn(1, 1, "c2r.prerotator")            # (b)
+_c2r_postrotator = _fn(2, 1, "c2r.postrotator")          # (m)
+_r2c_prerotator = _fn(3, 1, "r2c.prerotator")            # (m)
+_r2c_postrotator = _fn(4, 2, "r2c.postrotator")          # (b, m)
+_c2r_shuffle = _fn(10, 4, "c2r.shuffle")                 # (m, n, c, k)
+_c2r_long_shuffle = _fn(11, 4, "c2r.long_shuffle")       # (m, n, c, k)
+_r2c_shuffle = _fn(12, 4, "r2c.shuffle")                 # (m, n, c, k)
+_c2r_fused_preop = _fn(20, 2, "c2r.fused_preop")         # (m, b)
+_c2r_fused_postop = _fn(21, 3, "c2r.fused_postop")       # (m, n, c)
+_r2c_fused_preop = _fn(22, 4, "r2c.fused_preop")         # (a, c, m, q)
+_r2c_fused_postop = _fn(23, 2, "r2c.fused_postop")       # (m, b)
+_c2r_postpermuter = _fn(30, 3, "c2r.postpermuter")       # (m, n, c)
+_r2c_prepermuter = _fn(31, 3, "r2c.prepermuter")         # (m, n, c)
+
+
+def _call_pass(cfn, fn: Functor, d3, d2, d1, data, elem_bytes=None, stream=None):
+    p, eb, st = _resolve(data, elem_bytes, stream)
+    prm = params(fn.params)
+    check(cfn(fn.kind, prm, len(fn.params), p, int(d3), int(d2), int(d1), eb, st))
+
+
+def rotate(fn, d3, d2, d1, data, *, elem_bytes=None, stream=None):
+    """new[i][j] = old[(i + r(j)) mod d2][j] for every slice (src/rotate.cu:237-270)."""
+    _call_pass(lib().t213_rotate, fn, d3, d2, d1, data, elem_bytes, stream)
+
+
+def shuffle_fn(data, d3, d2, d1, fn, *, elem_bytes=None, stream=None):
+    """new[i][j] = old[i][s_i(j)] (src/shuffle.cu:66-76, src/skinny.cu:237-280)."""
+    _call_pass(lib().t213_row_shuffle, fn, d3, d2, d1, data, elem_bytes, stream)
+
+
+def col_shuffle_fn(fn, d3, d2, d1, data, *, elem_bytes=None, stream=None):
+    """new[i][j] = old[f(i,j)][j] (src/col_shuffle.cu:30-42, src/skinny.cu:282-309)."""
+    _call_pass(lib().t213_col_shuffle, fn, d3, d2, d1, data, elem_bytes, stream)
+
+
+def scatter_permute(fn, d3, d2, d1, data, *, elem_bytes=None, stream=None):
+    """new[p(i)][*] = old[i][*] along precomputed cycles (src/permute.cu:116-137)."""
+    _call_pass(lib().t213_scatter_permute, fn, d3, d2, d1, data, elem_bytes, stream)
+
+
+def _shape_call(cfn, data, d1, d2, d3, elem_bytes=None, stream=None):
+    p, eb, st = _resolve(data, elem_bytes, stream)
+    check(cfn(p, int(d1), int(d2), int(d3), eb, st))
+
+
+def transpose(data, d1, d2, d3, *, elem_bytes=None, stream=None):
+    """In-place 213 transpose of a (d1,d2,d3) array (src/transpose.cu:99-124)."""
+    _shape_call(lib().t213_transpose, data, d1, d2, d3, elem_bytes, stream)
+
+
+def c2r_transpose(data, d1, d2, d3, *, elem_bytes=None, stream=None):
+    """C2R on each d2 x d1 slice (src/transpose.cu:30-47)."""
+    _shape_call(lib().t213_c2r_transpose, data, d1, d2, d3, elem_bytes, stream)
+
+
+def r2c_transpose(data, d1, d2, d3, *, elem_bytes=None, stream=None):
+    """R2C, the inverse of c2r_transpose(d1, d2) (src/transpose.cu:70-89)."""
+    _shape_call(lib().t213_r2c_transpose, data, d1, d2, d3, elem_bytes, stream)
+
+
+def skinny_c2r_transpose(data, d1, d2, d3, *, elem_bytes=None, stream=None):
+    """Skinny C2R, d2 <= 32 (src/skinny.cu:313-333)."""
+    _shape_call(lib().t213_skinny_c2r_transpose, data, d1, d2, d3, elem_bytes, stream)
+
+
+def skinny_r2c_transpose(data, d1, d2, d3, *, elem_bytes=None, stream=None):
+    """Skinny R2C, d2 <= 32 (src/skinny.cu:344-363)."""
+    _shape_call(lib().t213_skinny_r2c_transpose, data, d1, d2, d3, elem_bytes, stream)
+
+
+def transpose_with_plan(data, d1, d2, d3, plan, t=0, *, elem_bytes=None, stream=None):
+    """The 213 transpose with an explicit plan family ('c2r', 'r2c', 'skinny',
+    'blocks', 'bands', 'bands_t', 'identity' or 'auto') and block/band size t."""
+    kind = _lib.PLAN_NAMES[plan] if isinstance(plan, str) else int(plan)
+    p, eb, st = _resolve(data, elem_bytes, stream)
+    check(lib().t213_transpose_with_plan(p, int(d1), int(d2), int(d3), eb, kind, int(t), st))
+
+
+def transpose_host(data, d1, d2, d3, *, elem_bytes=None, stream=None):
+    """End-to-end transpose of a host buffer (torch CPU tensor, numpy array or
+    raw pointer): copy in, transpose, copy out.  Synchronous."""
+    if hasattr(data, "data_ptr") and not getattr(data, "is_cuda", False):
+        ptr, eb = data.data_ptr(), data.element_size() if elem_bytes is None else elem_bytes
+    elif hasattr(data, "ctypes"):
+        ptr, eb = data.ctypes.data, data.itemsize if elem_bytes is None else elem_bytes
+    else:
+        ptr, eb = int(data), int(elem_bytes)
+    st = ctypes.c_void_p(int(getattr(stream, "cuda_stream", stream) or 0))
+    check(lib().t213_transpose_host(ctypes.c_void_p(ptr), int(d1), int(d2), int(d3), int(eb), st))
+
+
+def describe(d1, d2, d3, elem_bytes, plan="auto", t=0) -> str:
+    kind = _lib.PLAN_NAMES[plan] if isinstance(plan, str) else int(plan)
+    buf = ctypes.create_string_buffer(1024)
+    check(lib().t213_plan_describe(int(d1), int(d2), int(d3), int(elem_bytes), kind, int(t), buf, 1024))
+    return buf.value.decode()
+
+
+def plan_launches(d1, d2, d3, elem_bytes, plan="auto", t=0) -> int:
+    kind = _lib.PLAN_NAMES[plan] if isinstance(plan, str) else int(plan)
+    n = ctypes.c_int32(0)
+    check(lib().t213_plan_launches(int(d1), int(d2), int(d3), int(elem_bytes), kind, int(t), ctypes.byref(n)))
+    return int(n.value)
+
+
+class pass_timing:
+    """Per-pass CUDA-event timing of everything run while enabled."""
+
+    @staticmethod
+    def enable(on=True):
+        check(lib().t213_pass_timing_enable(1 if on else 0))
+
+    @staticmethod
+    def reset():
+        check(lib().t213_pass_timing_reset())
+
+    @staticmethod
+    def read(name):
+        ms, n = ctypes.c_double(0), ctypes.c_int64(0)
+        check(lib().t213_pass_timing_read(name.encode(), ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
+
+
+def release_cache():
+    check(lib().t213_release_cache())
+
+
+inplace = SimpleNamespace(
+    transpose=transpose,
+    c2r=SimpleNamespace(transpose=c2r_transpose),
+    r2c=SimpleNamespace(transpose=r2c_transpose),
+    detail=SimpleNamespace(
+        rotate=rotate,
+        shuffle_fn=shuffle_fn,
+        col_shuffle_fn=col_shuffle_fn,
+        scatter_permute=scatter_permute,
+        c2r=SimpleNamespace(
+            prerotator=_c2r_prerotator, postrotator=_c2r_postrotator, shuffle=_c2r_shuffle,
+            long_shuffle=_c2r_long_shuffle, postpermuter=_c2r_postpermuter,
+            scatter_postpermuter=_r2c_prepermuter, fused_preop=_c2r_fused_preop,
+            fused_postop=_c2r_fused_postop, skinny_transpose=skinny_c2r_transpose),
+        r2c=SimpleNamespace(
+            prerotator=_r2c_prerotator, postrotator=_r2c_postrotator, shuffle=_r2c_shuffle,
+            prepermuter=_r2c_prepermuter, scatter_prepermuter=_c2r_postpermuter,
+            fused_preop=_r2c_fused_preop, fused_postop=_r2c_fused_postop,
+            skinny_transpose=skinny_r2c_transpose),
+    ),
+)

@@ -1,0 +1,230 @@
+// Index functors of the C2R / R2C decomposition (Catanzaro, Keller & Garland,
+// "A Decomposition for In-place Matrix Transposition", PPoPP 2014, as extended
+// by kaihsin/213transpose with a batch axis) and of the segment permutations
+// used by the block and band plans.
+//
+// Inside a slice the matrix has m rows and n columns, c = gcd(m,n), a = m/c,
+// b = n/c.  Every functor is templated on its index word U (uint32_t when the
+// host has checked that all intermediate values stay below 2^31, otherwise
+// uint64_t with values below 2^63) and is usable on host and device, so the
+// host computes cycle tables with exactly the device's arithmetic.
+//
+// Three shapes of functor:
+//   column gathers  src(i,j): new[i][j] = old[src(i,j)][j]
+//   row gathers     src(i,j): new[i][j] = old[i][src(i,j)]
+//   scatters        dst(p):   new[dst(p)] = old[p]   (p indexes whole segments)
+// Every gather result is reduced into range, so a functor built from
+// inconsistent parameters can only give a wrong permutation, never an
+// out-of-bounds access.
+#pragma once
+
+#include "common.cuh"
+
+namespace t213 {
+
+// ---------------------------------------------------------------- rotators --
+// Amounts r(j) of the four rotators of include/equations.h, each a function of
+// its own constructor parameters only.  RotGather turns one into the column
+// gather new[i][j] = old[(i + r(j)) mod m][j] of an m-row slice, reducing the
+// amount modulo m the way the reference's (i - r + d2) % d2 does.
+
+template <typename U>
+struct RotC2RPre {  // r = j / b                      equations.h:78-94
+  FastDiv<U> b;
+  RotC2RPre() = default;
+  __host__ explicit RotC2RPre(int64_t b_) : b(b_) {}
+  T213_HD U amount(U j) const { return b.div(j); }
+};
+
+template <typename U>
+struct RotC2RPost {  // r = j mod m                   equations.h:97-113
+  FastDiv<U> m;
+  RotC2RPost() = default;
+  __host__ explicit RotC2RPost(int64_t m_) : m(m_) {}
+  T213_HD U amount(U j) const { return m.mod(j); }
+};
+
+template <typename U>
+struct RotR2CPre {  // r = (m - j mod m) mod m        equations.h:159-176
+  FastDiv<U> m;
+  RotR2CPre() = default;
+  __host__ explicit RotR2CPre(int64_t m_) : m(m_) {}
+  T213_HD U amount(U j) const {
+    U jm = m.mod(j);
+    return jm ? m.get() - jm : 0;
+  }
+};
+
+template <typename U>
+struct RotR2CPost {  // r = 0 if j < b, m - j/b if j/b < m, else 2m - j/b   equations.h:196-222
+  FastDiv<U> b;
+  U m;
+  RotR2CPost() = default;
+  __host__ RotR2CPost(int64_t b_, int64_t m_) : b(b_), m((U)m_) {}
+  T213_HD U amount(U j) const {
+    U bd = b.div(j);
+    if (bd == 0) return 0;
+    if (bd < m) return m - bd;
+    return bd < m + m ? m + m - bd : 0;
+  }
+};
+
+template <typename U, typename R>
+struct RotGather {
+  R r;
+  FastDiv<U> m;
+  RotGather() = default;
+  __host__ RotGather(R r_, int64_t m_) : r(r_), m(m_) {}
+  T213_HD U operator()(U i, U j) const {
+    U a = r.amount(j);
+    if (a >= m.get()) a = m.mod(a);
+    U s = i + a;
+    return s >= m.get() ? s - m.get() : s;
+  }
+};
+
+// ------------------------------------------------------- column shufflers --
+
+template <typename U>
+struct ColC2RFusedPre {  // (i + j/b) mod m           skinny.h:12-26
+  FastDiv<U> m, b;
+  ColC2RFusedPre() = default;
+  __host__ ColC2RFusedPre(int64_t m_, int64_t b_) : m(m_), b(b_) {}
+  T213_HD U operator()(U i, U j) const { return m.mod(i + b.div(j)); }
+};
+
+template <typename U>
+struct ColC2RFusedPost {  // (i*n - i*c/m + j) mod m   skinny.h:69-78
+  FastDiv<U> m;
+  U n, c;
+  ColC2RFusedPost() = default;
+  __host__ ColC2RFusedPost(int64_t m_, int64_t n_, int64_t c_) : m(m_), n((U)n_), c((U)c_) {}
+  T213_HD U operator()(U i, U j) const {
+    U mm = m.get();
+    U t1 = m.mod(i * n);
+    U t2 = m.mod(m.div(i * c));
+    U v = t1 + (mm - t2) + m.mod(j);  // < 3m
+    return m.mod(v);
+  }
+};
+
+template <typename U>
+struct ColR2CFusedPre {  // p((i - j) mod m)           skinny.h:87-107
+  FastDiv<U> a, c, m;
+  U q;
+  ColR2CFusedPre() = default;
+  __host__ ColR2CFusedPre(int64_t a_, int64_t c_, int64_t m_, int64_t q_)
+      : a(a_), c(c_), m(m_), q((U)(q_ % (a_ > 0 ? a_ : 1))) {}
+  T213_HD U p(U idx) const {
+    U cm1 = c.get() - 1;
+    U t1 = a.get() * c.mod(cm1 * idx);
+    U t2 = a.mod(a.mod(c.div(cm1 + idx)) * q);
+    return t1 + t2;
+  }
+  T213_HD U operator()(U i, U j) const {
+    U mm = m.get();
+    U idx = m.mod(i + mm - m.mod(j));
+    U s = p(idx);
+    return s < mm ? s : m.mod(s);
+  }
+};
+
+template <typename U>
+struct ColR2CFusedPost {  // (i + m - j/b) mod m       skinny.h:109-117
+  FastDiv<U> m, b;
+  ColR2CFusedPost() = default;
+  __host__ ColR2CFusedPost(int64_t m_, int64_t b_) : m(m_), b(b_) {}
+  T213_HD U operator()(U i, U j) const { return m.mod(i + m.get() - m.mod(b.div(j))); }
+};
+
+// ----------------------------------------------------------- row shufflers --
+
+template <typename U>
+struct RowC2RShuffle {  // equations.h:12-54 (and the 64-bit long_shuffle, skinny.h:29-67)
+  FastDiv<U> c, b, n;
+  U m, k;
+  RowC2RShuffle() = default;
+  __host__ RowC2RShuffle(int64_t m_, int64_t n_, int64_t c_, int64_t k_)
+      : c(c_), b(n_ / (c_ > 0 ? c_ : 1)), n(n_), m((U)m_) {
+    int64_t bb = n_ / (c_ > 0 ? c_ : 1);
+    int64_t kk = bb > 0 ? k_ % bb : 0;
+    if (kk < 0) kk += bb;
+    k = (U)kk;
+  }
+  T213_HD U operator()(U i, U j) const {
+    U jc = c.mod(j);
+    // i - (j mod c) <= m - c, evaluated without unsigned wrap
+    bool low = i + c.get() <= m + jc;
+    U f = j + i * (n.get() - 1) + (low ? 0 : m);
+    U qq = c.div(f);
+    U rem = f - qq * c.get();
+    U s = b.mod(k * b.mod(qq)) + rem * b.get();
+    return s < n.get() ? s : n.mod(s);
+  }
+};
+
+template <typename U>
+struct RowR2CShuffle {  // equations.h:178-194
+  FastDiv<U> m, n, b;
+  RowR2CShuffle() = default;
+  __host__ RowR2CShuffle(int64_t m_, int64_t n_, int64_t c_) : m(m_), n(n_), b(n_ / (c_ > 0 ? c_ : 1)) {}
+  T213_HD U operator()(U i, U j) const {
+    U r = m.mod(b.div(j) + i) + j * m.get();
+    return n.mod(r);
+  }
+};
+
+// ------------------------------------------------------------ row scatters --
+// new[dst(i)][*] = old[i][*]
+
+template <typename U>
+struct PermC2RPost {  // (i*n - i/a) mod m            equations.h:115-128
+  FastDiv<U> m, a;
+  U n;
+  PermC2RPost() = default;
+  __host__ PermC2RPost(int64_t m_, int64_t n_, int64_t c_)
+      : m(m_), a(m_ / (c_ > 0 ? c_ : 1)), n((U)n_) {}
+  T213_HD U operator()(U i) const {
+    U mm = m.get();
+    U t = m.mod(i * n) + mm - m.mod(a.div(i));
+    return m.mod(t);
+  }
+};
+
+template <typename U>
+struct PermR2CPre {  // equations.h:134-157
+  FastDiv<U> c, a, m;
+  U q;
+  PermR2CPre() = default;
+  // q = inverse of b modulo a, computed by the host (extended Euclid).
+  __host__ PermR2CPre(int64_t m_, int64_t c_, int64_t q_)
+      : c(c_), a(m_ / (c_ > 0 ? c_ : 1)), m(m_), q((U)q_) {}
+  T213_HD U operator()(U i) const {
+    U cm1 = c.get() - 1;
+    U kk = c.mod(cm1 * i);
+    U l = c.div(cm1 + i);
+    U s = kk * a.get() + a.mod(a.mod(l) * q);
+    return s < m.get() ? s : m.mod(s);
+  }
+};
+
+// ------------------------------------------------------ segment permutation --
+// An [A][Mid][C] array of segments rearranged to [C][Mid][A]:
+//   p = (x*Mid + s)*C + y  ->  (y*Mid + s)*A + x.
+// Mid == 1 is the transposition of an A x C matrix of segments.
+template <typename U>
+struct SegPerm3 {
+  FastDiv<U> C, Mid;
+  U A, mid, cc;
+  SegPerm3() = default;
+  __host__ SegPerm3(int64_t A_, int64_t Mid_, int64_t C_) : C(C_), Mid(Mid_), A((U)A_), mid((U)Mid_), cc((U)C_) {}
+  T213_HD U operator()(U p) const {
+    U y = C.mod(p);
+    U t = C.div(p);
+    U s = Mid.mod(t);
+    U x = Mid.div(t);
+    return (y * mid + s) * A + x;
+  }
+};
+
+}  // namespace t213

@@ -1,0 +1,307 @@
+// Cycle tables (host) and the launch of the segment-cycle walkers.
+//
+// The host lists every non-trivial cycle of a segment permutation with a
+// visited bitmap (O(S) functor evaluations with the device's own arithmetic),
+// then cuts cycles longer than a target length into chunks so the walk
+// spreads over the whole GPU.  Tables are cached per permutation and device
+// and uploaded once; they are the "precomputed cycle leaders" of the pass.
+#include <algorithm>
+#include <cstdio>
+#include <list>
+#include <map>
+
+#include "internal.h"
+#include "k_cycles.cuh"
+
+namespace t213 {
+
+CycleTable::~CycleTable() {
+  if (!d_chunks && !d_carry_items) return;
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (cur != dev) cudaSetDevice(dev);
+  if (d_chunks) cudaFree(d_chunks);
+  if (d_carry_items) cudaFree(d_carry_items);
+  if (cur != dev) cudaSetDevice(cur);
+}
+
+namespace {
+
+struct Cyc {
+  int64_t start, len;
+};
+
+template <typename P>
+int walk_cycles(const P &dst, int64_t S, std::vector<Cyc> &cycles, int64_t &moved, int64_t &max_len) {
+  std::vector<uint64_t> seen((size_t)((S + 63) / 64), 0);
+  moved = 0;
+  max_len = 0;
+  for (int64_t p = 0; p < S; p++) {
+    if (seen[p >> 6] >> (p & 63) & 1) continue;
+    int64_t x = p, len = 0;
+    do {
+      if (x < 0 || x >= S || (seen[x >> 6] >> (x & 63) & 1)) {
+        set_error("segment map is not a permutation of its index range");
+        return T213_ERR_INVALID_ARGUMENT;
+      }
+      seen[x >> 6] |= 1ull << (x & 63);
+      x = (int64_t)dst(x);
+      len++;
+    } while (x != p);
+    if (len > 1) {
+      cycles.push_back({p, len});
+      moved += len;
+      max_len = std::max(max_len, len);
+    }
+  }
+  return T213_OK;
+}
+
+template <typename P>
+int chunk_cycles(const P &dst, const std::vector<Cyc> &cycles, int64_t moved, int64_t items_per_chunk,
+                 std::vector<Chunk> &chunks, std::vector<CarryItem> &carries) {
+  const DevInfo &d = dev_info();
+  // aim for ~8 walker items per resident team
+  const int64_t resident_teams = (int64_t)d.sms * 8;
+  const int64_t target_chunks = std::max<int64_t>(1, 8 * resident_teams / std::max<int64_t>(1, items_per_chunk));
+  const int64_t Lc = std::max<int64_t>(16, (moved + target_chunks - 1) / target_chunks);
+  for (const Cyc &c : cycles) {
+    if (c.len <= Lc) {
+      chunks.push_back({c.start, c.len, -1});
+      continue;
+    }
+    const int64_t nch = (c.len + Lc - 1) / Lc;
+    const int64_t each = (c.len + nch - 1) / nch;
+    int64_t x = c.start, done = 0;
+    while (done < c.len) {
+      const int64_t l = std::min(each, c.len - done);
+      const int64_t slot = (int64_t)carries.size();
+      carries.push_back({x, slot});
+      chunks.push_back({x, l, slot});
+      for (int64_t s = 0; s < l; s++) x = (int64_t)dst(x);
+      done += l;
+    }
+  }
+  std::stable_sort(chunks.begin(), chunks.end(), [](const Chunk &a, const Chunk &b) { return a.len > b.len; });
+  return T213_OK;
+}
+
+template <typename U, typename Fn>
+bool with_perm(const PermSpec &p, Fn &&fn) {
+  if (p.kind == 0) return fn(SegPerm3<U>(p.A, p.Mid, p.C));
+  if (p.kind == T213_FN_C2R_POSTPERMUTER) return fn(PermC2RPost<U>(p.fn.p[0], p.fn.p[1], p.fn.p[2]));
+  if (p.kind == T213_FN_R2C_PREPERMUTER) {
+    // q = inverse of b = n/c modulo a = m/c (src/transpose.cu:77-82)
+    int64_t m = p.fn.p[0], n = p.fn.p[1], c = p.fn.p[2];
+    if (c <= 0) c = 1;
+    int64_t a = m / c, b = n / c;
+    // extended Euclid for b^{-1} mod a
+    int64_t x = 0, lastx = 1, aa = b, bb = a;
+    while (bb != 0) {
+      int64_t q = aa / bb, nb = aa % bb;
+      aa = bb;
+      bb = nb;
+      int64_t nx = lastx - q * x;
+      lastx = x;
+      x = nx;
+    }
+    int64_t q = (aa == 1) ? (lastx < 0 ? lastx + a : lastx) : 0;
+    return fn(PermR2CPre<U>(m, c, q));
+  }
+  return false;
+}
+
+bool perm_fits32(const PermSpec &p) {
+  if (p.kind == 0) {
+    double s = (double)p.A * (double)p.Mid * (double)p.C;
+    return s < (double)(1ll << 31);
+  }
+  return fits32(p.fn, p.fn.p[0], p.fn.p[1]);
+}
+
+struct Key {
+  PermSpec spec;
+  int64_t ipc;
+  int dev;
+};
+
+std::mutex g_mu;
+std::list<std::pair<Key, std::shared_ptr<CycleTable>>> g_cache;  // front = most recent
+constexpr size_t kCacheMax = 64;
+
+}  // namespace
+
+std::shared_ptr<CycleTable> get_cycle_table(const PermSpec &p, int64_t items_per_chunk, int *status) {
+  *status = T213_OK;
+  const int dev = dev_info().id;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (auto it = g_cache.begin(); it != g_cache.end(); ++it) {
+      if (it->first.dev == dev && it->first.ipc == items_per_chunk && it->first.spec == p) {
+        auto v = it->second;
+        g_cache.splice(g_cache.begin(), g_cache, it);
+        return v;
+      }
+    }
+  }
+  std::vector<Cyc> cycles;
+  std::vector<Chunk> chunks;
+  std::vector<CarryItem> carries;
+  int64_t moved = 0, max_len = 0;
+  int rc = T213_OK;
+  bool ok;
+  auto build = [&](auto fn) -> bool {
+    rc = walk_cycles(fn, p.S, cycles, moved, max_len);
+    if (rc == T213_OK) rc = chunk_cycles(fn, cycles, moved, items_per_chunk, chunks, carries);
+    return true;
+  };
+  if (perm_fits32(p))
+    ok = with_perm<uint32_t>(p, build);
+  else
+    ok = with_perm<uint64_t>(p, build);
+  if (!ok) {
+    set_error("unknown segment permutation kind");
+    *status = T213_ERR_INVALID_ARGUMENT;
+    return nullptr;
+  }
+  if (rc != T213_OK) {
+    *status = rc;
+    return nullptr;
+  }
+  auto ct = std::make_shared<CycleTable>();
+  ct->spec = p;
+  ct->dev = dev;
+  ct->n_chunks = (int64_t)chunks.size();
+  ct->n_carry = (int64_t)carries.size();
+  ct->moved = moved;
+  ct->n_cycles = (int64_t)cycles.size();
+  ct->max_len = max_len;
+  ct->h_chunks.assign((const char *)chunks.data(), (const char *)(chunks.data() + chunks.size()));
+  ct->h_carry_items.assign((const char *)carries.data(), (const char *)(carries.data() + carries.size()));
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_cache.push_front({Key{p, items_per_chunk, dev}, ct});
+    while (g_cache.size() > kCacheMax) g_cache.pop_back();
+  }
+  return ct;
+}
+
+int CycleTable::ensure_uploaded() {
+  std::lock_guard<std::mutex> lk(mu);
+  if (n_chunks == 0 || d_chunks) return T213_OK;
+  cudaError_t e = cudaMalloc(&d_chunks, h_chunks.size());
+  if (e == cudaSuccess) e = cudaMemcpy(d_chunks, h_chunks.data(), h_chunks.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && n_carry > 0) {
+    e = cudaMalloc(&d_carry_items, h_carry_items.size());
+    if (e == cudaSuccess)
+      e = cudaMemcpy(d_carry_items, h_carry_items.data(), h_carry_items.size(), cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    if (d_chunks) cudaFree(d_chunks);
+    if (d_carry_items) cudaFree(d_carry_items);
+    d_chunks = d_carry_items = nullptr;
+    return cuda_status(e, "cycle table upload");
+  }
+  return T213_OK;
+}
+
+int seg_cycles_team(int64_t seg_bytes, int aw) {
+  int64_t words = seg_bytes / aw;
+  int64_t team = (words + 31) / 32 * 32;
+  return (int)std::max<int64_t>(32, std::min<int64_t>(kCycleThreads, team));
+}
+
+size_t seg_cycles_carry_bytes(const CycleTable &ct, int64_t d3, int64_t seg_bytes) {
+  return (size_t)(ct.n_carry * d3 * seg_bytes);
+}
+
+int launch_seg_cycles(const CycleTable &ct, char *data, int64_t d3, int64_t slice_bytes, int64_t seg_bytes,
+                      cudaStream_t st, LaunchStats *ls, char *carry_override, size_t carry_override_bytes) {
+  if (ct.n_chunks == 0 || d3 <= 0) return T213_OK;
+  {
+    int up = const_cast<CycleTable &>(ct).ensure_uploaded();
+    if (up) return up;
+  }
+  const int aw = seg_access_width(data, seg_bytes, slice_bytes);
+  const int team = seg_cycles_team(seg_bytes, aw);
+  const int64_t words = seg_bytes / aw;
+  const int64_t pieces = (words + team - 1) / team;
+  const DevInfo &d = dev_info();
+  int status = T213_OK;
+  char *carry = nullptr;
+  const size_t cb = seg_cycles_carry_bytes(ct, d3, seg_bytes);
+  if (ct.n_carry > 0) {
+    if (carry_override) {
+      if (carry_override_bytes < cb) {
+        set_error("carry buffer too small");
+        return T213_ERR_INVALID_ARGUMENT;
+      }
+      carry = carry_override;
+    } else {
+      carry = workspace(st, cb, &status);
+      if (!carry) return status;
+    }
+  }
+  bool ok = false;
+  auto run_aw = [&](auto AWc) -> bool {
+    constexpr int AW = decltype(AWc)::value;
+    if (ct.n_carry > 0) {
+      const int64_t total = ct.n_carry * d3 * (seg_bytes / AW);
+      int64_t grid = std::min<int64_t>((int64_t)d.sms * 8, (total + kCycleThreads - 1) / kCycleThreads);
+      k_carry_save<AW><<<(unsigned)std::max<int64_t>(1, grid), kCycleThreads, 0, st>>>(
+          data, slice_bytes, d3, seg_bytes, (const CarryItem *)ct.d_carry_items, ct.n_carry, carry);
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) {
+        status = cuda_status(e, "k_carry_save launch");
+        return true;
+      }
+      if (ls) ls->launches++;
+    }
+    auto go = [&](auto UT) -> bool {
+      using U = decltype(UT);
+      return with_perm<U>(ct.spec, [&](auto dst) -> bool {
+        using P = decltype(dst);
+        const int64_t items = ct.n_chunks * pieces * d3;
+        const int64_t threads_needed = items * team;
+        int64_t grid = std::min<int64_t>((int64_t)d.sms * (d.max_threads_sm / kCycleThreads),
+                                         (threads_needed + kCycleThreads - 1) / kCycleThreads);
+        grid = std::max<int64_t>(1, grid);
+        k_seg_cycles<AW, 8, P, U><<<(unsigned)grid, kCycleThreads, 0, st>>>(
+            data, slice_bytes, d3, seg_bytes, team, pieces, (const Chunk *)ct.d_chunks, ct.n_chunks, carry, dst);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) status = cuda_status(e, "k_seg_cycles launch");
+        if (ls) ls->launches++;
+        return true;
+      });
+    };
+    if (perm_fits32(ct.spec))
+      ok = go(uint32_t{});
+    else
+      ok = go(uint64_t{});
+    return true;
+  };
+  switch (aw) {
+    case 16:
+      run_aw(IC<16>{});
+      break;
+    case 8:
+      run_aw(IC<8>{});
+      break;
+    case 4:
+      run_aw(IC<4>{});
+      break;
+    case 2:
+      run_aw(IC<2>{});
+      break;
+    default:
+      run_aw(IC<1>{});
+      break;
+  }
+  if (!ok && status == T213_OK) {
+    set_error("unknown segment permutation kind");
+    return T213_ERR_INVALID_ARGUMENT;
+  }
+  return status;
+}
+
+}  // namespace t213

@@ -1,0 +1,107 @@
+// Launchers of the square-block tile swaps and of the band transposes.
+#include <algorithm>
+
+#include "internal.h"
+#include "k_tiles.cuh"
+
+namespace t213 {
+
+namespace {
+
+template <typename Kern>
+int64_t resident_grid(Kern kern, int threads, size_t smem, int64_t units) {
+  const DevInfo &d = dev_info();
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return std::max<int64_t>(1, std::min<int64_t>((int64_t)per_sm * d.sms, units));
+}
+
+constexpr int64_t kBandSmemCap = 200 * 1024;
+
+}  // namespace
+
+int64_t band_smem_limit() { return kBandSmemCap; }
+
+int64_t band_smem_bytes(int64_t R, int64_t C, int eb) {
+  const int64_t S = (C % 2 == 0) ? C + 1 : C;
+  return R * S * eb;
+}
+
+int launch_tile_swap(char *data, int64_t d3, int64_t m, int64_t n, int64_t t, int eb, cudaStream_t st,
+                     LaunchStats *ls) {
+  if (t <= 0 || m % t || n % t) {
+    set_error("block size must divide both matrix sides");
+    return T213_ERR_INVALID_ARGUMENT;
+  }
+  if (d3 <= 0 || m <= 0 || n <= 0) return T213_OK;
+  const int64_t Bm = m / t, Bn = n / t;
+  auto go = [&](auto EBc, auto TSc) -> int {
+    constexpr int EB = decltype(EBc)::value;
+    constexpr int TS = decltype(TSc)::value;
+    const int64_t nt = (t + TS - 1) / TS;
+    const int64_t units = d3 * Bm * Bn * (nt * (nt + 1) / 2);
+    auto kern = k_tile_swap<EB, TS>;
+    const int64_t grid = resident_grid(kern, kTileThreads, 0, units);
+    kern<<<(unsigned)grid, kTileThreads, 0, st>>>(data, n, m * n, d3, t, Bm, Bn, nt);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e, "k_tile_swap launch");
+    if (ls) ls->launches++;
+    return T213_OK;
+  };
+  switch (eb) {
+    case 1:
+      return go(IC<1>{}, IC<64>{});
+    case 2:
+      return go(IC<2>{}, IC<64>{});
+    case 4:
+      return go(IC<4>{}, IC<32>{});
+    case 8:
+      return go(IC<8>{}, IC<32>{});
+    case 16:
+      return go(IC<16>{}, IC<16>{});
+  }
+  set_error("unsupported element size");
+  return T213_ERR_UNSUPPORTED;
+}
+
+int launch_band_transpose(char *data, int64_t n_bands, int64_t R, int64_t C, int eb, cudaStream_t st,
+                          LaunchStats *ls) {
+  if (n_bands <= 0 || R <= 0 || C <= 0) return T213_OK;
+  const int64_t smem = band_smem_bytes(R, C, eb);
+  if (smem > kBandSmemCap || R * C >= (1ll << 31)) {
+    set_error("band does not fit shared memory");
+    return T213_ERR_UNSUPPORTED;
+  }
+  const uint32_t S = (uint32_t)((C % 2 == 0) ? C + 1 : C);
+  auto go = [&](auto EBc) -> int {
+    constexpr int EB = decltype(EBc)::value;
+    auto kern = k_band_transpose<EB>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(band)");
+    const int64_t grid = resident_grid(kern, kTileThreads, (size_t)smem, n_bands);
+    kern<<<(unsigned)grid, kTileThreads, (size_t)smem, st>>>(data, n_bands, (uint32_t)R, (uint32_t)C, S,
+                                                            FastDiv<uint32_t>((uint64_t)C),
+                                                            FastDiv<uint32_t>((uint64_t)R));
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e, "k_band_transpose launch");
+    if (ls) ls->launches++;
+    return T213_OK;
+  };
+  switch (eb) {
+    case 1:
+      return go(IC<1>{});
+    case 2:
+      return go(IC<2>{});
+    case 4:
+      return go(IC<4>{});
+    case 8:
+      return go(IC<8>{});
+    case 16:
+      return go(IC<16>{});
+  }
+  set_error("unsupported element size");
+  return T213_ERR_UNSUPPORTED;
+}
+
+}  // namespace t213
