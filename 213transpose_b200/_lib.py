@@ -74,6 +74,7 @@ _SIGS = {
     "t213_pass_timing_read": ([ctypes.c_char_p, ctypes.POINTER(ctypes.c_double), _pi64], ctypes.c_int),
     "t213_pass_timing_reset": ([], ctypes.c_int),
     "t213_release_cache": ([], ctypes.c_int),
+    "t213_device_status": ([_vp, ctypes.POINTER(_i32)], ctypes.c_int),
     "t213_batch_create": ([ctypes.POINTER(TensorDesc), _i32, ctypes.POINTER(_vp)], ctypes.c_int),
     "t213_batch_execute": ([_vp, _vp], ctypes.c_int),
     "t213_batch_status": ([_vp, _vp], ctypes.c_int),

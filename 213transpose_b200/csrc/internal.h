@@ -32,6 +32,10 @@ struct DevInfo {
 };
 const DevInfo &dev_info();  // the current device, cached
 
+// Per-device status word written by kernels whose bounded waits ran out
+// (T213_ERR_TIMEOUT); read and cleared by t213_device_status.
+int *device_status_word(int *status);
+
 // ------------------------------------------------------------- workspace --
 // Grow-only scratch buffer per (device, stream).  Calls on one stream run in
 // order, so they can share it; calls on different streams never do.

@@ -22,6 +22,7 @@
 
 #include "common.cuh"
 #include "functors.cuh"
+#include "tma.cuh"
 
 namespace t213 {
 
@@ -117,6 +118,104 @@ __global__ void __launch_bounds__(kCycleThreads)
     const W v = __ldcg(reinterpret_cast<const W *>(data + k * slice_bytes + ci.pos * seg_bytes) + w);
     reinterpret_cast<W *>(carry + (ci.slot * d3 + k) * seg_bytes)[w] = v;
   }
+}
+
+// ---------------------------------------------------------------------------
+// TMA walker for segments of 16-byte multiples.  One walker per 32-thread CTA;
+// lane 0 drives a ring of NB shared-memory buffers with bulk asynchronous
+// copies (cp.async.bulk): the piece at x_i is loaded into buffer i % NB, and
+// step k stores buffer (k-1) % NB to x_k once x_k's own old value has landed.
+// Loads run NB-2 positions ahead of the stores; a buffer is reloaded only
+// after the bulk store that read it has finished reading (wait_group.read).
+// Every mbarrier wait is bounded; on timeout the walker records
+// T213_ERR_TIMEOUT in *status, drains its stores and returns.
+// ---------------------------------------------------------------------------
+constexpr int kBulkRing = 6;
+
+template <typename P, typename U>
+__global__ void __launch_bounds__(32)
+    k_seg_cycles_bulk(char *__restrict__ data, int64_t slice_bytes, int64_t d3, int64_t seg_bytes,
+                      int64_t piece_bytes, int64_t pieces, const Chunk *__restrict__ chunks, int64_t n_chunks,
+                      const char *__restrict__ carry, P dst, int *status) {
+  constexpr int NB = kBulkRing;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+  char *buf = reinterpret_cast<char *>(smem_raw) + 128;
+  if (threadIdx.x != 0) return;
+  for (int i = 0; i < NB; i++) mbar_init(&bars[i], 1);
+  fence_barrier_init();
+  uint32_t parity = 0;  // bit b: parity of the next completion of bars[b]
+  bool failed = false;
+  const int64_t per_chunk = pieces * d3;
+  const int64_t items = n_chunks * per_chunk;
+  for (int64_t it = blockIdx.x; it < items && !failed; it += gridDim.x) {
+    const int64_t c = it / per_chunk;
+    const int64_t rest = it - c * per_chunk;
+    const int64_t k = rest / pieces;
+    const int64_t pc = rest - k * pieces;
+    const Chunk ch = chunks[c];
+    const int64_t off = pc * piece_bytes;
+    const uint32_t pb = (uint32_t)min(piece_bytes, seg_bytes - off);
+    char *base = data + k * slice_bytes + off;
+    const int64_t L = ch.len;
+    U xi = (U)ch.start;  // position of the newest load issued
+    U pos[NB];
+    // x_0: from the carry slot (split chunk) or from memory (whole cycle)
+    mbar_expect_tx(&bars[0], pb);
+    if (ch.carry >= 0)
+      bulk_g2s(buf, carry + (ch.carry * d3 + k) * seg_bytes + off, pb, &bars[0]);
+    else
+      bulk_g2s(buf, base + (int64_t)xi * seg_bytes, pb, &bars[0]);
+    pos[0] = xi;
+    int64_t issued = 1;
+    while (issued < L && issued <= NB - 2) {
+      xi = dst(xi);
+      const int b = (int)(issued % NB);
+      pos[b] = xi;
+      mbar_expect_tx(&bars[b], pb);
+      bulk_g2s(buf + (int64_t)b * piece_bytes, base + (int64_t)xi * seg_bytes, pb, &bars[b]);
+      issued++;
+    }
+    // old value of x_0 in place
+    if (!mbar_wait(&bars[0], parity & 1u)) {
+      failed = true;
+      break;
+    }
+    parity ^= 1u;
+    U last = pos[0];
+    for (int64_t s = 1; s <= L; s++) {
+      const int bs = (int)(s % NB);
+      const int bp = (int)((s - 1) % NB);
+      U target;
+      if (s < L) {
+        // x_s must be read before it is overwritten
+        if (!mbar_wait(&bars[bs], (parity >> bs) & 1u)) {
+          failed = true;
+          break;
+        }
+        parity ^= 1u << bs;
+        target = pos[bs];
+      } else {
+        target = dst(last);  // cycle start or the next chunk's start
+      }
+      fence_proxy_async();
+      bulk_s2g(base + (int64_t)target * seg_bytes, buf + (int64_t)bp * piece_bytes, pb);
+      bulk_commit();
+      last = target;
+      if (issued < L) {
+        bulk_wait_read<1>();  // the buffer's previous store has read it
+        xi = dst(xi);
+        const int b = (int)(issued % NB);
+        pos[b] = xi;
+        mbar_expect_tx(&bars[b], pb);
+        bulk_g2s(buf + (int64_t)b * piece_bytes, base + (int64_t)xi * seg_bytes, pb, &bars[b]);
+        issued++;
+      }
+    }
+    bulk_wait_read<0>();
+  }
+  bulk_wait_all<0>();
+  if (failed) atomicExch(status, 5 /* T213_ERR_TIMEOUT */);
 }
 
 }  // namespace t213

@@ -19,6 +19,7 @@
 
 #include "common.cuh"
 #include "functors.cuh"
+#include "tma.cuh"
 
 namespace t213 {
 
@@ -69,8 +70,14 @@ __global__ void __launch_bounds__(kGatherThreads)
       const W *g = reinterpret_cast<const W *>(ubase + e_lo * EB);
       W *s = reinterpret_cast<W *>(sm);
       const uint32_t nw = (e_hi > e_lo) ? (uint32_t)((e_hi - e_lo) / PER) : 0u;
+      if constexpr (AW >= 4) {
 #pragma unroll 4
-      for (uint32_t w = threadIdx.x; w < nw; w += blockDim.x) s[w] = __ldcs(g + w);
+        for (uint32_t w = threadIdx.x; w < nw; w += blockDim.x) cp_async<AW>(s + w, g + w);
+        cp_async_wait_all();
+      } else {
+#pragma unroll 4
+        for (uint32_t w = threadIdx.x; w < nw; w += blockDim.x) s[w] = __ldcs(g + w);
+      }
     }
     if (CLUSTER)
       cg::this_cluster().sync();
@@ -183,8 +190,12 @@ __global__ void __launch_bounds__(kGatherThreads)
         uint32_t r = t / (uint32_t)wpr;
         uint32_t w = t - r * (uint32_t)wpr;
         const Wd *gp = reinterpret_cast<const Wd *>(sbase + (int64_t)(row_lo + r) * pitch) + w;
-        reinterpret_cast<Wd *>(sm + (int64_t)r * WS)[w] = __ldcs(gp);
+        if constexpr (AW >= 4)
+          cp_async<AW>(reinterpret_cast<Wd *>(sm + (int64_t)r * WS) + w, gp);
+        else
+          reinterpret_cast<Wd *>(sm + (int64_t)r * WS)[w] = __ldcs(gp);
       }
+      if constexpr (AW >= 4) cp_async_wait_all();
     }
     if (CLUSTER)
       cg::this_cluster().sync();

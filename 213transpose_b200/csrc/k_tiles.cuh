@@ -69,6 +69,111 @@ __global__ void __launch_bounds__(kTileThreads)
   }
 }
 
+// Vectorised tile swap for 4-, 8- and 16-byte elements and blocks whose side
+// is a multiple of 32: tiles are 32 x 32 elements, every global access is a
+// 16-byte vector (a tile row is RV = 2*EB vectors), shared memory rows have a
+// stride of 33 elements so both the row-wise fill and the column-wise drain
+// are free of bank conflicts, and the vectors of the next tile pair are loaded
+// into registers before the current pair is written back, so each thread
+// keeps two pairs of loads in flight.
+template <int EB>
+struct TileVec {
+  static constexpr int RV = 2 * EB;            // 16-byte vectors per tile row
+  static constexpr int PE = 16 / EB;           // elements per vector
+  static constexpr int VPT = (32 * RV) / kTileThreads;  // vectors per thread per tile
+};
+
+template <int EB>
+__global__ void __launch_bounds__(kTileThreads)
+    k_tile_swap_vec(char *__restrict__ data, int64_t n, int64_t slice_elems, int64_t d3, int64_t t,
+                    int64_t Bm, int64_t Bn, int64_t nt) {
+  using E = typename ElemT<EB>::type;
+  constexpr int RV = TileVec<EB>::RV, PE = TileVec<EB>::PE, VPT = TileVec<EB>::VPT;
+  constexpr int S = 33;
+  __shared__ E tA[32 * S];
+  __shared__ E tB[32 * S];
+  union V {
+    uint4 v;
+    E e[PE];
+  };
+  const int64_t pairs = nt * (nt + 1) / 2;
+  const int64_t per_slice = Bm * Bn * pairs;
+  const int64_t total = d3 * per_slice;
+  E *d = reinterpret_cast<E *>(data);
+
+  auto origin = [&](int64_t u, int64_t &ar, int64_t &ac, bool &diag) -> E * {
+    const int64_t k = u / per_slice;
+    const int64_t r = u - k * per_slice;
+    const int64_t blk = r / pairs;
+    const int64_t p = r - blk * pairs;
+    const int64_t I = blk / Bn, J = blk - I * Bn;
+    int64_t x, y;
+    tri_decode(p, nt, x, y);
+    ar = x * 32;
+    ac = y * 32;
+    diag = (x == y);
+    return d + k * slice_elems + (I * t) * n + J * t;
+  };
+  auto load = [&](E *s, int64_t ar, int64_t ac, bool diag, V (&ra)[VPT], V (&rb)[VPT]) {
+#pragma unroll
+    for (int q = 0; q < VPT; q++) {
+      const int v = threadIdx.x + q * kTileThreads;
+      const int r = v / RV, ch = v % RV;
+      ra[q].v = __ldcs(reinterpret_cast<const uint4 *>(s + (ar + r) * n + ac) + ch);
+      if (!diag) rb[q].v = __ldcs(reinterpret_cast<const uint4 *>(s + (ac + r) * n + ar) + ch);
+    }
+  };
+
+  int64_t u = blockIdx.x;
+  if (u >= total) return;
+  V na[VPT], nb[VPT];
+  int64_t ar, ac;
+  bool diag;
+  E *s = origin(u, ar, ac, diag);
+  load(s, ar, ac, diag, na, nb);
+  for (; u < total; u += gridDim.x) {
+    V ca[VPT], cb[VPT];
+#pragma unroll
+    for (int q = 0; q < VPT; q++) {
+      ca[q] = na[q];
+      cb[q] = nb[q];
+    }
+    E *cs = s;
+    const int64_t car = ar, cac = ac;
+    const bool cdiag = diag;
+    if (u + gridDim.x < total) {
+      s = origin(u + gridDim.x, ar, ac, diag);
+      load(s, ar, ac, diag, na, nb);  // in flight while this pair is written back
+    }
+#pragma unroll
+    for (int q = 0; q < VPT; q++) {
+      const int v = threadIdx.x + q * kTileThreads;
+      const int r = v / RV, ch = v % RV;
+#pragma unroll
+      for (int e = 0; e < PE; e++) {
+        tA[r * S + ch * PE + e] = ca[q].e[e];
+        if (!cdiag) tB[r * S + ch * PE + e] = cb[q].e[e];
+      }
+    }
+    __syncthreads();
+    // row w of A^T (column w of A) goes to B's place and vice versa
+#pragma unroll
+    for (int q = 0; q < VPT; q++) {
+      const int v = threadIdx.x + q * kTileThreads;
+      const int w = v / RV, ch = v % RV;
+      V oa, ob;
+#pragma unroll
+      for (int e = 0; e < PE; e++) {
+        oa.e[e] = tA[(ch * PE + e) * S + w];
+        if (!cdiag) ob.e[e] = tB[(ch * PE + e) * S + w];
+      }
+      __stcs(reinterpret_cast<uint4 *>(cs + (cac + w) * n + car) + ch, oa.v);
+      if (!cdiag) __stcs(reinterpret_cast<uint4 *>(cs + (car + w) * n + cac) + ch, ob.v);
+    }
+    __syncthreads();
+  }
+}
+
 // Bands: contiguous R x C row-major blocks -> C x R.  Shared memory holds the
 // band with row stride S = C + (C even) so the column-wise read is free of
 // bank conflicts.

@@ -243,6 +243,52 @@ int launch_seg_cycles(const CycleTable &ct, char *data, int64_t d3, int64_t slic
     }
   }
   bool ok = false;
+  if (aw == 16 && seg_bytes >= 1024) {
+    // TMA bulk walker: pieces of up to 16 KB, a ring of kBulkRing buffers
+    const int64_t piece = std::min<int64_t>(seg_bytes, 16 * 1024);
+    const int64_t npieces = (seg_bytes + piece - 1) / piece;
+    const int64_t smem = 128 + (int64_t)kBulkRing * piece;
+    int *stw = device_status_word(&status);
+    if (!stw) return status;
+    if (ct.n_carry > 0) {
+      const int64_t total = ct.n_carry * d3 * (seg_bytes / 16);
+      int64_t grid = std::min<int64_t>((int64_t)d.sms * 8, (total + kCycleThreads - 1) / kCycleThreads);
+      k_carry_save<16><<<(unsigned)std::max<int64_t>(1, grid), kCycleThreads, 0, st>>>(
+          data, slice_bytes, d3, seg_bytes, (const CarryItem *)ct.d_carry_items, ct.n_carry, carry);
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_status(e, "k_carry_save launch");
+      if (ls) ls->launches++;
+    }
+    auto go = [&](auto UT) -> bool {
+      using U = decltype(UT);
+      return with_perm<U>(ct.spec, [&](auto dst) -> bool {
+        using P = decltype(dst);
+        auto kern = k_seg_cycles_bulk<P, U>;
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) {
+          status = cuda_status(e, "cudaFuncSetAttribute(bulk walker)");
+          return true;
+        }
+        int per_sm = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32, (size_t)smem) != cudaSuccess || per_sm < 1)
+          per_sm = 1;
+        const int64_t items = ct.n_chunks * npieces * d3;
+        const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((int64_t)per_sm * d.sms, items));
+        kern<<<(unsigned)grid, 32, (size_t)smem, st>>>(data, slice_bytes, d3, seg_bytes, piece, npieces,
+                                                      (const Chunk *)ct.d_chunks, ct.n_chunks, carry, dst, stw);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) status = cuda_status(e, "k_seg_cycles_bulk launch");
+        if (ls) ls->launches++;
+        return true;
+      });
+    };
+    ok = perm_fits32(ct.spec) ? go(uint32_t{}) : go(uint64_t{});
+    if (!ok && status == T213_OK) {
+      set_error("unknown segment permutation kind");
+      return T213_ERR_INVALID_ARGUMENT;
+    }
+    return status;
+  }
   auto run_aw = [&](auto AWc) -> bool {
     constexpr int AW = decltype(AWc)::value;
     if (ct.n_carry > 0) {

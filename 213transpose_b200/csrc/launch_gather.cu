@@ -76,30 +76,36 @@ struct ColCfg {
 ColCfg col_config(int64_t m, int64_t n, int eb, const void *data) {
   ColCfg c;
   c.aw = pick_aw(eb, data, n * eb, 0);
-  const int64_t per = c.aw / eb;
-  if (n % per) c.aw = eb;  // (cannot happen: aw == 16 implies n*eb % 16 == 0)
   const int64_t P = c.aw / eb;
-  const int64_t wmin = std::max<int64_t>(P, 128 / eb);
-  for (int64_t wbytes : {(int64_t)128, (int64_t)64, (int64_t)32, (int64_t)16}) {
+  auto strip = [&](int64_t wbytes, bool widen) -> int64_t {
     int64_t W = std::max<int64_t>(P, wbytes / eb);
-    if (wbytes < 128 && W >= wmin) continue;
-    // widen short strips so a unit is worth ~48 KB
-    if (wbytes == 128) {
+    if (widen) {  // short columns: widen so a unit is worth ~48 KB
       int64_t want = (48 * 1024) / std::max<int64_t>(1, m * eb);
       if (want > W) W = want / W * W;
     }
     W = std::min<int64_t>(W, round_up(n, P));
-    W = round_up(W, P);
-    const int64_t WS = (W * eb) % 128 == 0 ? W + P : W;
-    const int64_t bytes = m * WS * eb;
-    if (bytes <= kSmemCap) {
+    return round_up(W, P);
+  };
+  auto stride = [&](int64_t W) { return (W * eb) % 128 == 0 ? W + P : W; };
+  // 1) one CTA holds the whole strip: the widest strip that fits
+  for (int64_t wbytes : {(int64_t)128, (int64_t)64, (int64_t)32, (int64_t)16}) {
+    const int64_t W = strip(wbytes, wbytes == 128);
+    if (wbytes < 128 && W * eb > wbytes && W > P) continue;
+    const int64_t WS = stride(W);
+    if (m * WS * eb <= kSmemCap) {
       c.W = W;
       c.WS = WS;
       c.K = 1;
       c.H = m;
-      c.smem = bytes;
+      c.smem = m * WS * eb;
       return c;
     }
+  }
+  // 2) a thread-block cluster shares a 128-byte strip through DSMEM
+  for (int64_t wbytes : {(int64_t)128, (int64_t)32}) {
+    const int64_t W = strip(wbytes, false);
+    const int64_t WS = stride(W);
+    const int64_t bytes = m * WS * eb;
     int K = (int)((bytes + kSmemTarget - 1) / kSmemTarget);
     if (K > kMaxCluster) K = (int)((bytes + kSmemCap - 1) / kSmemCap);
     if (K <= kMaxCluster) {
@@ -111,7 +117,7 @@ ColCfg col_config(int64_t m, int64_t n, int eb, const void *data) {
       return c;
     }
   }
-  // scratch fallback: copy groups of columns to the workspace
+  // 3) scratch fallback: copy groups of columns to the workspace
   c.K = 0;
   c.W = std::max<int64_t>(P, 128 / eb);
   c.group_w = std::max<int64_t>(c.W, (int64_t)(256ll << 20) / std::max<int64_t>(1, m * eb) / c.W * c.W);

@@ -36,6 +36,24 @@ int launch_tile_swap(char *data, int64_t d3, int64_t m, int64_t n, int64_t t, in
   }
   if (d3 <= 0 || m <= 0 || n <= 0) return T213_OK;
   const int64_t Bm = m / t, Bn = n / t;
+  const bool vec_ok = (eb >= 4) && (t % 32 == 0) && (((uintptr_t)data | (uint64_t)(n * eb)) % 16 == 0);
+  if (vec_ok) {
+    auto gov = [&](auto EBc) -> int {
+      constexpr int EB = decltype(EBc)::value;
+      const int64_t nt = t / 32;
+      const int64_t units = d3 * Bm * Bn * (nt * (nt + 1) / 2);
+      auto kern = k_tile_swap_vec<EB>;
+      const int64_t grid = resident_grid(kern, kTileThreads, 0, units);
+      kern<<<(unsigned)grid, kTileThreads, 0, st>>>(data, n, m * n, d3, t, Bm, Bn, nt);
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_status(e, "k_tile_swap_vec launch");
+      if (ls) ls->launches++;
+      return T213_OK;
+    };
+    if (eb == 4) return gov(IC<4>{});
+    if (eb == 8) return gov(IC<8>{});
+    return gov(IC<16>{});
+  }
   auto go = [&](auto EBc, auto TSc) -> int {
     constexpr int EB = decltype(EBc)::value;
     constexpr int TS = decltype(TSc)::value;

@@ -77,6 +77,24 @@ char *workspace(cudaStream_t st, size_t bytes, int *status) {
   return p;
 }
 
+int *device_status_word(int *status) {
+  static std::mutex mu;
+  static std::map<int, int *> words;
+  const int dev = dev_info().id;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = words.find(dev);
+  if (it != words.end()) return it->second;
+  int *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, 256);
+  if (e == cudaSuccess) e = cudaMemset(p, 0, 256);
+  if (e != cudaSuccess) {
+    *status = cuda_status(e, "status word");
+    return nullptr;
+  }
+  words[dev] = p;
+  return p;
+}
+
 static void release_workspaces() {
   const int dev = dev_info().id;
   std::lock_guard<std::mutex> lk(g_ws_mu);
@@ -935,6 +953,20 @@ int t213_plan_launches(int64_t d1, int64_t d2, int64_t d3, int32_t elem_bytes, i
     }
   }
   *launches = n;
+  return T213_OK;
+}
+
+int t213_device_status(t213_stream_t stream, int32_t *device_status) {
+  if (!device_status) return T213_ERR_INVALID_ARGUMENT;
+  int rc = T213_OK;
+  int *w = device_status_word(&rc);
+  if (!w) return rc;
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_status(e, "cudaStreamSynchronize");
+  int v = 0;
+  if ((e = cudaMemcpy(&v, w, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) return cuda_status(e, "status read");
+  if (v) cudaMemset(w, 0, sizeof(int));
+  *device_status = v;
   return T213_OK;
 }
 

@@ -168,6 +168,10 @@ int t213_plan_launches(int64_t d1, int64_t d2, int64_t d3, int32_t elem_bytes, i
 int t213_pass_timing_enable(int32_t enable);
 int t213_pass_timing_read(const char *pass_name, double *total_ms, int64_t *launches);
 int t213_pass_timing_reset(void);
+/* Synchronises the stream, then returns (and clears) the device's status word:
+ * T213_OK, or T213_ERR_TIMEOUT if a kernel's bounded wait on an asynchronous
+ * copy ran out since the last read. */
+int t213_device_status(t213_stream_t stream, int32_t *device_status);
 /* Frees cached plans and workspace on the current device. */
 int t213_release_cache(void);
 

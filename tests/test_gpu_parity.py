@@ -50,7 +50,8 @@ def test_transpose_random(cuda, oracle, t213, shape, eb):
 
 
 PLAN_SHAPES = [(64, 48, 2), (512, 384, 2), (100, 37, 1), (37, 100, 2), (600, 45, 1), (45, 600, 2),
-               (1000, 999, 1), (128, 96, 3), (96, 128, 3), (4096, 30, 1), (30, 4096, 1), (300, 300, 2)]
+               (1000, 999, 1), (128, 96, 3), (96, 128, 3), (4096, 30, 1), (30, 4096, 1), (300, 300, 2),
+               (3000, 2000, 2), (2000, 3000, 1), (2048, 1536, 2), (6144, 32, 2), (32, 6144, 2)]
 
 
 @pytest.mark.parametrize("eb", (4, 8, 16, 1))
