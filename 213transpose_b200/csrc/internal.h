@@ -108,6 +108,7 @@ int launch_band_transpose(char *data, int64_t n_bands, int64_t R, int64_t C, int
                           LaunchStats *ls);
 int64_t band_smem_bytes(int64_t R, int64_t C, int eb);
 int64_t band_smem_limit();
+bool band_fits(int64_t R, int64_t C, int eb);
 
 // ------------------------------------------------------------ cycle tables --
 // A permutation of segment indices: either a segment 3-D rearrangement

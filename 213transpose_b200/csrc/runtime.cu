@@ -328,8 +328,8 @@ int64_t pick_band_t(int64_t m, int64_t n, int eb) {
   return largest_divisor_le(m, band_smem_limit() / per_row);
 }
 int64_t pick_band_t_t(int64_t m, int64_t n, int eb) {
-  // t | n, band m x t fits shared memory: m * (t+1) * eb <= limit
-  int64_t lim = band_smem_limit() / std::max<int64_t>(1, m * eb) - 1;
+  // t | n, band m x t fits shared memory
+  int64_t lim = band_smem_limit() / std::max<int64_t>(1, m * eb);
   if (lim < 1) return 0;
   return largest_divisor_le(n, lim);
 }
@@ -389,7 +389,7 @@ int build_plan(Plan &P, int kind, int64_t t) {
     }
     case T213_PLAN_BANDS: {
       if (t <= 0) t = pick_band_t(m, n, eb);
-      if (t <= 0 || m % t || band_smem_bytes(t, n, eb) > band_smem_limit()) {
+      if (t <= 0 || m % t || !band_fits(t, n, eb)) {
         set_error("band size must divide d2 and a t x d1 band must fit shared memory");
         return T213_ERR_UNSUPPORTED;
       }
@@ -410,7 +410,7 @@ int build_plan(Plan &P, int kind, int64_t t) {
     }
     case T213_PLAN_BANDS_T: {
       if (t <= 0) t = pick_band_t_t(m, n, eb);
-      if (t <= 0 || n % t || band_smem_bytes(m, t, eb) > band_smem_limit()) {
+      if (t <= 0 || n % t || !band_fits(m, t, eb)) {
         set_error("band size must divide d1 and a d2 x t band must fit shared memory");
         return T213_ERR_UNSUPPORTED;
       }
