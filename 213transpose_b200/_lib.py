@@ -81,6 +81,7 @@ _SIGS = {
     "t213_batch_describe": ([_vp, ctypes.c_char_p, _sz], ctypes.c_int),
     "t213_batch_destroy": ([_vp], ctypes.c_int),
     "t213_transpose_looped": ([ctypes.POINTER(TensorDesc), _i32, _vp], ctypes.c_int),
+    "t213_batch_tune": ([ctypes.POINTER(TensorDesc), _i32, _vp], ctypes.c_int),
     "t213_tune_shape": ([_vp, _i64, _i64, _i64, _i32, _vp, ctypes.POINTER(_i32), _pi64], ctypes.c_int),
     "t213_tuner_load": ([ctypes.c_char_p], ctypes.c_int),
     "t213_tuner_save": ([ctypes.c_char_p], ctypes.c_int),

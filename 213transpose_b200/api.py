@@ -204,6 +204,72 @@ class pass_timing:
         return ms.value, n.value
 
 
+class Batch:
+    """Many tensors transposed by one persistent, graph-captured launch
+    (t213_batch_*).  `tensors` is a list of (data, d1, d2, d3) or
+    (data, d1, d2, d3, elem_bytes[, plan]) tuples; data are CUDA tensors or raw
+    device pointers (then elem_bytes is required)."""
+
+    def __init__(self, tensors, tune=False):
+        descs = []
+        self._keep = []
+        for t in tensors:
+            data, d1, d2, d3 = t[:4]
+            eb = t[4] if len(t) > 4 else None
+            plan = t[5] if len(t) > 5 else "auto"
+            p, eb, _ = _resolve(data, eb, 0)
+            kind = _lib.PLAN_NAMES[plan] if isinstance(plan, str) else int(plan)
+            descs.append(_lib.TensorDesc(p.value, int(d1), int(d2), int(d3), int(eb), kind))
+            self._keep.append(data)
+        self.count = len(descs)
+        self._descs = (_lib.TensorDesc * max(1, self.count))(*descs)
+        if tune:
+            check(lib().t213_batch_tune(self._descs, self.count, _stream_of(None)))
+        h = ctypes.c_void_p(0)
+        check(lib().t213_batch_create(self._descs, self.count, ctypes.byref(h)))
+        self._h = h
+
+    def execute(self, stream=None):
+        st = _stream_of(stream)
+        check(lib().t213_batch_execute(self._h, st))
+
+    def looped(self, stream=None):
+        """The baseline: the plain call looped over the same list."""
+        check(lib().t213_transpose_looped(self._descs, self.count, _stream_of(stream)))
+
+    def status(self, stream=None) -> int:
+        return int(lib().t213_batch_status(self._h, _stream_of(stream)))
+
+    def describe(self) -> str:
+        buf = ctypes.create_string_buffer(512)
+        check(lib().t213_batch_describe(self._h, buf, 512))
+        return buf.value.decode()
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().t213_batch_destroy(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _stream_of(stream):
+    if stream is None:
+        torch = _t()
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return ctypes.c_void_p(int(getattr(stream, "cuda_stream", stream)))
+
+
+def device_status(stream=None) -> int:
+    v = ctypes.c_int32(0)
+    check(lib().t213_device_status(_stream_of(stream), ctypes.byref(v)))
+    return int(v.value)
+
+
 def release_cache():
     check(lib().t213_release_cache())
 

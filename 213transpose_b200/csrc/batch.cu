@@ -1,11 +1,167 @@
-// Batched form (persistent executor) — first build: the looped baseline only.
+// Batched form: many tensors of uneven shape and element size transposed by
+// one persistent kernel launch (k_batch), captured in a CUDA graph on the
+// first execute and replayed after that.  No reference counterpart: the
+// reference offers only a loop of plain calls (t213_transpose_looped here).
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <tuple>
+
+#include "k_batch.cuh"
 #include "plan.h"
 
 using namespace t213;
 
 struct t213_batch_st {
-  int dummy;
+  int dev = 0;
+  std::vector<t213_tensor_desc> tensors;
+  std::vector<std::shared_ptr<Plan>> plans;
+  std::vector<BPass> h_passes;
+  std::vector<BItem> h_items;
+  // tensors run by their own plans as graph nodes after the persistent kernel:
+  // larger than the direct threshold (bandwidth-bound on their own) or with a
+  // plan that does not fit the persistent kernel's shared memory
+  std::vector<int> spill;
+  BPass *d_passes = nullptr;
+  BItem *d_items = nullptr;
+  unsigned long long *d_ctrs = nullptr;  // one per pass, then the queue head
+  int *d_status = nullptr;
+  char *d_carry = nullptr;
+  size_t carry_bytes = 0;
+  int n_ctrs = 0;
+  int grid = 0;
+  size_t spill_ws = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t graph_stream = nullptr;
+  std::string desc;
+  int64_t total_bytes = 0;
 };
+
+namespace {
+
+constexpr int64_t kItemBytes = 1024 * 1024;  // target bytes read per queue item
+
+// Tensors above this size saturate the GPU on their own and keep their
+// specialised kernels (graph nodes); smaller ones share the persistent kernel.
+int64_t direct_threshold() {
+  static int64_t v = [] {
+    const char *e = getenv("T213_BATCH_DIRECT_MB");
+    return (int64_t)((e ? atof(e) : 32.0) * (1 << 20));
+  }();
+  return v;
+}
+
+int aw_for(int eb, const void *data, int64_t pitch) {
+  if (eb >= 16) return 16;
+  if (eb >= 4 && ((((uintptr_t)data) | (uint64_t)pitch) % 16 == 0)) return 16;
+  return eb;
+}
+
+template <typename U>
+bool set_col_fn(AnyFn<U> &a, const FnSpec &f, int64_t m) {
+  switch (f.kind) {
+    case T213_FN_C2R_PREROTATOR:
+      a.set(f.kind, RotGather<U, RotC2RPre<U>>(RotC2RPre<U>(f.p[0]), m));
+      return true;
+    case T213_FN_C2R_POSTROTATOR:
+      a.set(f.kind, RotGather<U, RotC2RPost<U>>(RotC2RPost<U>(f.p[0]), m));
+      return true;
+    case T213_FN_R2C_PREROTATOR:
+      a.set(f.kind, RotGather<U, RotR2CPre<U>>(RotR2CPre<U>(f.p[0]), m));
+      return true;
+    case T213_FN_R2C_POSTROTATOR:
+      a.set(f.kind, RotGather<U, RotR2CPost<U>>(RotR2CPost<U>(f.p[0], f.p[1]), m));
+      return true;
+    case T213_FN_C2R_FUSED_PREOP:
+      a.set(f.kind, ColC2RFusedPre<U>(f.p[0], f.p[1]));
+      return true;
+    case T213_FN_C2R_FUSED_POSTOP:
+      a.set(f.kind, ColC2RFusedPost<U>(f.p[0], f.p[1], f.p[2]));
+      return true;
+    case T213_FN_R2C_FUSED_PREOP:
+      a.set(f.kind, ColR2CFusedPre<U>(f.p[0], f.p[1], f.p[2], f.p[3]));
+      return true;
+    case T213_FN_R2C_FUSED_POSTOP:
+      a.set(f.kind, ColR2CFusedPost<U>(f.p[0], f.p[1]));
+      return true;
+  }
+  return false;
+}
+
+template <typename U>
+bool set_row_fn(AnyFn<U> &a, const FnSpec &f) {
+  if (f.kind == T213_FN_R2C_SHUFFLE) {
+    a.set(f.kind, RowR2CShuffle<U>(f.p[0], f.p[1], f.p[2]));
+    return true;
+  }
+  if (f.kind == T213_FN_C2R_SHUFFLE || f.kind == T213_FN_C2R_LONG_SHUFFLE) {
+    a.set(f.kind, RowC2RShuffle<U>(f.p[0], f.p[1], f.p[2], f.p[3]));
+    return true;
+  }
+  return false;
+}
+
+template <typename U>
+bool set_perm_fn(AnyFn<U> &a, const PermSpec &p) {
+  if (p.kind == 0) {
+    a.set(0, SegPerm3<U>(p.A, p.Mid, p.C));
+    return true;
+  }
+  if (p.kind == T213_FN_C2R_POSTPERMUTER) {
+    a.set(p.kind, PermC2RPost<U>(p.fn.p[0], p.fn.p[1], p.fn.p[2]));
+    return true;
+  }
+  if (p.kind == T213_FN_R2C_PREPERMUTER) {
+    int64_t m = p.fn.p[0], n = p.fn.p[1], c = p.fn.p[2] > 0 ? p.fn.p[2] : 1, q;
+    ext_gcd(n / c, m / c, &q);
+    a.set(p.kind, PermR2CPre<U>(m, c, q));
+    return true;
+  }
+  return false;
+}
+
+// Column strip width for the batch kernel (single CTA, <= kBatchSmem).
+bool batch_col_cfg(int64_t m, int64_t n, int eb, int aw, int64_t &W, int64_t &WS) {
+  const int64_t P = aw / eb;
+  for (int64_t wbytes : {(int64_t)128, (int64_t)64, (int64_t)32, (int64_t)16}) {
+    W = std::max<int64_t>(P, wbytes / eb);
+    if (wbytes == 128) {
+      int64_t want = (32 * 1024) / std::max<int64_t>(1, m * eb);
+      if (want > W) W = want / W * W;
+    }
+    W = std::min<int64_t>(W, (n + P - 1) / P * P);
+    W = (W + P - 1) / P * P;
+    WS = (W * eb) % 128 == 0 ? W + P : W;
+    if (m * WS * eb <= kBatchHalf) return true;
+  }
+  return false;
+}
+
+bool plan_fits_batch(const Plan &p) {
+  for (const PassDesc &q : p.passes) {
+    switch (q.type) {
+      case PT_COL: {
+        int64_t W, WS;
+        if (!batch_col_cfg(q.m, q.n, p.eb, p.eb, W, WS)) return false;
+        break;
+      }
+      case PT_ROW:
+        if (q.n * p.eb > kBatchHalf) return false;
+        break;
+      case PT_BAND:
+        if (q.R * q.C * p.eb > kBatchHalf) return false;
+        break;
+      default:
+        break;
+    }
+  }
+  return true;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -21,10 +177,389 @@ int t213_transpose_looped(const t213_tensor_desc *tensors, int32_t count, t213_s
   return T213_OK;
 }
 
-int t213_batch_create(const t213_tensor_desc *, int32_t, t213_batch *) { return T213_ERR_UNSUPPORTED; }
-int t213_batch_execute(t213_batch, t213_stream_t) { return T213_ERR_UNSUPPORTED; }
-int t213_batch_status(t213_batch, t213_stream_t) { return T213_ERR_UNSUPPORTED; }
-int t213_batch_describe(t213_batch, char *, size_t) { return T213_ERR_UNSUPPORTED; }
-int t213_batch_destroy(t213_batch) { return T213_OK; }
+int t213_batch_create(const t213_tensor_desc *tensors, int32_t count, t213_batch *out) {
+  if (!out || count < 0 || (count > 0 && !tensors)) {
+    set_error("t213_batch_create: bad arguments");
+    return T213_ERR_INVALID_ARGUMENT;
+  }
+  *out = nullptr;
+  auto *B = new t213_batch_st();
+  B->dev = dev_info().id;
+  B->tensors.assign(tensors, tensors + count);
+  int rc = T213_OK;
+  auto fail = [&](int code) {
+    t213_batch_destroy(B);
+    return code;
+  };
+
+  // ---- plans ---------------------------------------------------------------
+  std::vector<int> per_tensor_first_pass(count, -1), per_tensor_npass(count, 0);
+  std::vector<std::vector<int>> tensor_passes(count);
+  for (int32_t i = 0; i < count; i++) {
+    const t213_tensor_desc &d = tensors[i];
+    if (d.d1 < 0 || d.d2 < 0 || d.d3 < 0 || (d.elem_bytes != 1 && d.elem_bytes != 2 && d.elem_bytes != 4 &&
+                                              d.elem_bytes != 8 && d.elem_bytes != 16)) {
+      set_error("t213_batch_create: bad tensor descriptor");
+      return fail(T213_ERR_INVALID_ARGUMENT);
+    }
+    if (d.d1 * d.d2 * d.d3 > 0 && !d.data) {
+      set_error("t213_batch_create: NULL data");
+      return fail(T213_ERR_INVALID_ARGUMENT);
+    }
+    B->total_bytes += d.d1 * d.d2 * d.d3 * d.elem_bytes;
+    std::shared_ptr<Plan> P;
+    if (d.d1 * d.d2 * d.d3 > 0) {
+      P = get_plan(d.d1, d.d2, d.d3, d.elem_bytes, d.plan_kind, 0, &rc);
+      if (!P) return fail(rc);
+      if (!plan_fits_batch(*P) && d.plan_kind == T213_PLAN_AUTO) {
+        // another family that fits the persistent kernel's shared memory
+        for (int k : {T213_PLAN_BLOCKS, T213_PLAN_BANDS, T213_PLAN_BANDS_T, T213_PLAN_C2R, T213_PLAN_R2C}) {
+          int rc2 = T213_OK;
+          auto Q = get_plan(d.d1, d.d2, d.d3, d.elem_bytes, k, 0, &rc2);
+          if (Q && plan_fits_batch(*Q)) {
+            P = Q;
+            break;
+          }
+        }
+      }
+      if (!plan_fits_batch(*P) || d.d1 * d.d2 * d.d3 * d.elem_bytes > direct_threshold()) B->spill.push_back(i);
+    }
+    B->plans.push_back(P);
+  }
+
+  // ---- passes ------------------------------------------------------------------
+  size_t carry_total = 0;
+  std::vector<size_t> carry_off;
+  for (int32_t i = 0; i < count; i++) {
+    const t213_tensor_desc &d = tensors[i];
+    const std::shared_ptr<Plan> &P = B->plans[i];
+    if (!P || std::find(B->spill.begin(), B->spill.end(), i) != B->spill.end()) continue;
+    const int eb = d.elem_bytes;
+    char *data = (char *)d.data;
+    const int64_t slice_bytes = d.d1 * d.d2 * eb;
+    for (const PassDesc &q : P->passes) {
+      BPass bp;
+      bp.eb = eb;
+      bp.data = data;
+      bp.d3 = d.d3;
+      bp.slice_bytes = slice_bytes;
+      bp.m = q.m;
+      bp.n = q.n;
+      switch (q.type) {
+        case PT_TILE: {
+          bp.kind = BK_TILE;
+          bp.t = q.t;
+          bp.Bm = q.m / q.t;
+          bp.Bn = q.n / q.t;
+          bp.nt = (q.t + 31) / 32;
+          bp.pairs = bp.nt * (bp.nt + 1) / 2;
+          bp.tile_vec = eb >= 4 && q.t % 32 == 0 && ((((uintptr_t)data) | (uint64_t)(q.n * eb)) % 16 == 0);
+          bp.n_units = d.d3 * bp.Bm * bp.Bn * bp.pairs;
+          break;
+        }
+        case PT_BAND: {
+          bp.kind = BK_BAND;
+          bp.R = q.R;
+          bp.C = q.C;
+          const int Q = 16 / eb;
+          bp.band_vec = eb >= 2 && eb <= 8 && q.R % Q == 0 && q.C % Q == 0 && ((uintptr_t)data % 16 == 0);
+          bp.n_units = d.d3 * q.bands;
+          break;
+        }
+        case PT_COL: {
+          bp.kind = BK_COL;
+          bp.aw = aw_for(eb, data, q.n * eb);
+          int64_t W, WS;
+          if (!batch_col_cfg(q.m, q.n, eb, bp.aw, W, WS)) {
+            bp.aw = eb;  // narrowest access width always fits (checked by plan_fits_batch)
+            batch_col_cfg(q.m, q.n, eb, bp.aw, W, WS);
+          }
+          bp.W = W;
+          bp.WS = WS;
+          bp.n_strips = (q.n + W - 1) / W;
+          bp.n_units = d.d3 * bp.n_strips;
+          bp.u64 = !fits32(q.fn, q.m, q.n);
+          if (bp.u64)
+            set_col_fn<uint64_t>(bp.f64, q.fn, q.m);
+          else
+            set_col_fn<uint32_t>(bp.f32, q.fn, q.m);
+          break;
+        }
+        case PT_ROW: {
+          bp.kind = BK_ROW;
+          bp.aw = aw_for(eb, data, q.n * eb);
+          bp.rows_per_unit = std::max<int64_t>(1, std::min<int64_t>(q.m, (64 * 1024) / std::max<int64_t>(1, q.n * eb)));
+          bp.n_units = (d.d3 * q.m + bp.rows_per_unit - 1) / bp.rows_per_unit;
+          bp.u64 = !fits32(q.fn, q.m, q.n);
+          if (bp.u64)
+            set_row_fn<uint64_t>(bp.f64, q.fn);
+          else
+            set_row_fn<uint32_t>(bp.f32, q.fn);
+          break;
+        }
+        case PT_SEG: {
+          const CycleTable &ct = *q.table;
+          if ((rc = const_cast<CycleTable &>(ct).ensure_uploaded())) return fail(rc);
+          bp.seg_bytes = q.seg_bytes;
+          bp.seg_aw = seg_access_width(data, q.seg_bytes, slice_bytes);
+          bp.chunks = (const Chunk *)ct.d_chunks;
+          bp.carries = (const CarryItem *)ct.d_carry_items;
+          bp.n_chunks = ct.n_chunks;
+          bp.n_carry = ct.n_carry;
+          bp.u64 = !(q.perm.kind == 0 ? (double)q.perm.S < 2.0e9 : fits32(q.perm.fn, q.perm.fn.p[0], q.perm.fn.p[1]));
+          if (bp.u64)
+            set_perm_fn<uint64_t>(bp.f64, q.perm);
+          else
+            set_perm_fn<uint32_t>(bp.f32, q.perm);
+          if (ct.n_carry > 0) {
+            BPass cp = bp;
+            cp.kind = BK_CARRY;
+            cp.n_units = ct.n_carry * d.d3;
+            B->h_passes.push_back(cp);
+            tensor_passes[i].push_back((int)B->h_passes.size() - 1);
+            carry_off.push_back(carry_total);
+            carry_total += (size_t)(ct.n_carry * d.d3 * q.seg_bytes + 255) / 256 * 256;
+          }
+          bp.kind = BK_SEG;
+          bp.seg_tma = bp.seg_aw == 16 && q.seg_bytes >= 512;
+          bp.piece_bytes = bp.seg_tma ? std::min<int64_t>(q.seg_bytes, kBatchPiece) : 32 * bp.seg_aw;
+          bp.pieces = (q.seg_bytes + bp.piece_bytes - 1) / bp.piece_bytes;
+          bp.n_units = ct.n_chunks * bp.pieces * d.d3;
+          if (ct.n_carry > 0) carry_off.push_back(carry_off.back());  // same buffer as its CARRY pass
+          break;
+        }
+      }
+      if (bp.n_units == 0) continue;
+      B->h_passes.push_back(bp);
+      tensor_passes[i].push_back((int)B->h_passes.size() - 1);
+    }
+  }
+  // carry pool
+  if (carry_total > 0) {
+    cudaError_t e = cudaMalloc(&B->d_carry, carry_total);
+    if (e != cudaSuccess) return fail(cuda_status(e, "batch carry pool"));
+    B->carry_bytes = carry_total;
+    size_t ci = 0;
+    for (BPass &bp : B->h_passes)
+      if ((bp.kind == BK_CARRY || bp.kind == BK_SEG) && bp.n_carry > 0) bp.carry_buf = B->d_carry + carry_off[ci++];
+  }
+
+  // ---- items, level by level -------------------------------------------------------
+  B->n_ctrs = (int)B->h_passes.size();
+  std::vector<int64_t> items_of_pass(B->h_passes.size(), 0);
+  size_t max_levels = 0;
+  for (auto &tp : tensor_passes) max_levels = std::max(max_levels, tp.size());
+  for (size_t lvl = 0; lvl < max_levels; lvl++) {
+    for (int32_t i = 0; i < count; i++) {
+      if (lvl >= tensor_passes[i].size()) continue;
+      const int pi = tensor_passes[i][lvl];
+      BPass &bp = B->h_passes[pi];
+      bp.done_ctr = pi;
+      if (lvl > 0) {
+        const int prev = tensor_passes[i][lvl - 1];
+        bp.dep_ctr = prev;
+        bp.dep_target = items_of_pass[prev];
+      }
+      // units per item: about kItemBytes read per item
+      int64_t upi = 1;
+      const int eb = bp.eb;
+      auto per = [&](int64_t unit_bytes) { return std::max<int64_t>(1, kItemBytes / std::max<int64_t>(1, unit_bytes)); };
+      switch (bp.kind) {
+        case BK_TILE:
+          upi = per(2 * 32 * 32 * eb);
+          break;
+        case BK_BAND:
+          upi = per(bp.R * bp.C * eb);
+          break;
+        case BK_COL:
+          upi = per(bp.m * bp.W * eb);
+          break;
+        case BK_ROW:
+          upi = per(bp.rows_per_unit * bp.n * eb);
+          break;
+        case BK_CARRY:
+          upi = per(bp.seg_bytes);
+          break;
+        case BK_SEG: {
+          const int64_t avg_len = std::max<int64_t>(1, (bp.n_chunks ? (B->plans[i]->passes.empty() ? 1 : 1) : 1));
+          (void)avg_len;
+          upi = std::max<int64_t>(kBatchWarps, per(bp.piece_bytes * 8) / kBatchWarps * kBatchWarps);
+          break;
+        }
+      }
+      for (int64_t u = 0; u < bp.n_units; u += upi) {
+        B->h_items.push_back(BItem{pi, 0, u, std::min(bp.n_units, u + upi)});
+        items_of_pass[pi]++;
+      }
+    }
+  }
+
+  // ---- upload --------------------------------------------------------------
+  cudaError_t e = cudaSuccess;
+  if (!B->h_passes.empty()) {
+    e = cudaMalloc(&B->d_passes, B->h_passes.size() * sizeof(BPass));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(B->d_passes, B->h_passes.data(), B->h_passes.size() * sizeof(BPass), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess && !B->h_items.empty()) {
+    e = cudaMalloc(&B->d_items, B->h_items.size() * sizeof(BItem));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(B->d_items, B->h_items.data(), B->h_items.size() * sizeof(BItem), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&B->d_ctrs, (B->n_ctrs + 1) * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&B->d_status, 256);
+  if (e == cudaSuccess) e = cudaMemset(B->d_status, 0, 256);
+  if (e != cudaSuccess) return fail(cuda_status(e, "batch upload"));
+  // workspace the spilled plans need during capture
+  for (int i : B->spill) B->spill_ws = std::max(B->spill_ws, plan_workspace_bytes(*B->plans[i]));
+  // grid: resident CTAs of the persistent kernel
+  e = cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(kBatchSmem + kBatchBarBytes));
+  if (e != cudaSuccess) return fail(cuda_status(e, "cudaFuncSetAttribute(k_batch)"));
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, kBatchThreads,
+                                                    (size_t)(kBatchSmem + kBatchBarBytes)) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  B->grid = per_sm * dev_info().sms;
+
+  char buf[256];
+  int64_t direct_bytes = 0;
+  for (int i : B->spill) direct_bytes += tensors[i].d1 * tensors[i].d2 * tensors[i].d3 * tensors[i].elem_bytes;
+  snprintf(buf, sizeof buf,
+           "batch: %d tensors, %.1f MB; persistent kernel: %d tensors, %zu passes, %zu items, grid %d x %d threads; "
+           "graph nodes: %d tensors, %.1f MB",
+           count, B->total_bytes / 1e6, count - (int)B->spill.size(), B->h_passes.size(), B->h_items.size(), B->grid,
+           kBatchThreads, (int)B->spill.size(), direct_bytes / 1e6);
+  B->desc = buf;
+  *out = B;
+  return T213_OK;
+}
+
+static int batch_enqueue(t213_batch B, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(B->d_ctrs, 0, (B->n_ctrs + 1) * sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return cuda_status(e, "batch counters reset");
+  if (!B->h_items.empty()) {
+    k_batch<<<B->grid, kBatchThreads, (size_t)(kBatchSmem + kBatchBarBytes), st>>>(
+        B->d_passes, B->d_items, (int64_t)B->h_items.size(), B->d_ctrs, B->d_ctrs + B->n_ctrs, B->d_status);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e, "k_batch launch");
+  }
+  for (int i : B->spill) {
+    int rc = run_plan(*B->plans[i], (char *)B->tensors[i].data, st, nullptr);
+    if (rc) return rc;
+  }
+  return T213_OK;
+}
+
+int t213_batch_execute(t213_batch B, t213_stream_t stream) {
+  if (!B) return T213_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (B->exec && B->graph_stream == st) {
+    cudaError_t e = cudaGraphLaunch(B->exec, st);
+    return e == cudaSuccess ? T213_OK : cuda_status(e, "cudaGraphLaunch");
+  }
+  // first execute on this stream: reserve what capture cannot allocate, capture
+  if (!B->spill.empty()) {
+    int rc = T213_OK;
+    if (B->spill_ws && !workspace(st, B->spill_ws, &rc)) return rc;
+    for (int i : B->spill)
+      for (const PassDesc &q : B->plans[i]->passes)
+        if (q.table && (rc = q.table->ensure_uploaded())) return rc;
+    int *w = device_status_word(&rc);
+    if (!w) return rc;
+  }
+  if (st == nullptr) {
+    // the legacy default stream cannot be captured: run without a graph
+    return batch_enqueue(B, st);
+  }
+  if (B->exec) {
+    cudaGraphExecDestroy(B->exec);
+    B->exec = nullptr;
+  }
+  if (B->graph) {
+    cudaGraphDestroy(B->graph);
+    B->graph = nullptr;
+  }
+  cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return cuda_status(e, "cudaStreamBeginCapture");
+  int rc = batch_enqueue(B, st);
+  cudaGraph_t g = nullptr;
+  e = cudaStreamEndCapture(st, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
+  B->graph = g;
+  e = cudaGraphInstantiate(&B->exec, g, 0);
+  if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
+  B->graph_stream = st;
+  e = cudaGraphLaunch(B->exec, st);
+  return e == cudaSuccess ? T213_OK : cuda_status(e, "cudaGraphLaunch");
+}
+
+int t213_batch_status(t213_batch B, t213_stream_t stream) {
+  if (!B) return T213_ERR_INVALID_ARGUMENT;
+  cudaError_t e = cudaStreamSynchronize((cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_status(e, "cudaStreamSynchronize");
+  int v = 0;
+  e = cudaMemcpy(&v, B->d_status, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_status(e, "batch status read");
+  if (v) {
+    cudaMemset(B->d_status, 0, sizeof(int));
+    set_error("a bounded wait of the persistent batch kernel ran out");
+  }
+  return v;
+}
+
+int t213_batch_tune(const t213_tensor_desc *tensors, int32_t count, t213_stream_t stream) {
+  if (count < 0 || (count > 0 && !tensors)) return T213_ERR_INVALID_ARGUMENT;
+  // every distinct shape once
+  std::map<std::tuple<int64_t, int64_t, int64_t, int>, int> rep;
+  for (int32_t i = 0; i < count; i++) {
+    const t213_tensor_desc &d = tensors[i];
+    if (d.d1 <= 1 || d.d2 <= 1 || d.d3 <= 0) continue;
+    rep.emplace(std::make_tuple(d.d1, d.d2, d.d3, d.elem_bytes), i);
+  }
+  int64_t maxb = 0;
+  for (auto &kv : rep) {
+    const t213_tensor_desc &d = tensors[kv.second];
+    maxb = std::max<int64_t>(maxb, d.d1 * d.d2 * d.d3 * d.elem_bytes);
+  }
+  if (rep.empty()) return T213_OK;
+  char *scratch = nullptr;
+  cudaError_t e = cudaMalloc(&scratch, (size_t)maxb);
+  if (e != cudaSuccess) return cuda_status(e, "tuning scratch");
+  int rc = T213_OK;
+  for (auto &kv : rep) {
+    const t213_tensor_desc &d = tensors[kv.second];
+    int32_t kind = 0;
+    int64_t t = 0;
+    rc = t213_tune_shape(scratch, d.d1, d.d2, d.d3, d.elem_bytes, stream, &kind, &t);
+    if (rc) break;
+  }
+  cudaStreamSynchronize((cudaStream_t)stream);
+  cudaFree(scratch);
+  return rc;
+}
+
+int t213_batch_describe(t213_batch B, char *buf, size_t buflen) {
+  if (!B || !buf || !buflen) return T213_ERR_INVALID_ARGUMENT;
+  snprintf(buf, buflen, "%s", B->desc.c_str());
+  return T213_OK;
+}
+
+int t213_batch_destroy(t213_batch B) {
+  if (!B) return T213_OK;
+  if (B->exec) cudaGraphExecDestroy(B->exec);
+  if (B->graph) cudaGraphDestroy(B->graph);
+  if (B->d_passes) cudaFree(B->d_passes);
+  if (B->d_items) cudaFree(B->d_items);
+  if (B->d_ctrs) cudaFree(B->d_ctrs);
+  if (B->d_status) cudaFree(B->d_status);
+  if (B->d_carry) cudaFree(B->d_carry);
+  delete B;
+  return T213_OK;
+}
 
 }  // extern "C"

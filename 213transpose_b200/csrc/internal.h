@@ -83,6 +83,12 @@ inline int seg_access_width(const void *base, int64_t seg_bytes, int64_t slice_b
   return 1;
 }
 
+// Per-kernel launch facts cached across calls: the shared-memory attribute is
+// set once per (kernel, bytes), and the resident-CTA count per SM is queried
+// once per (kernel, threads, bytes, cluster).
+bool kernel_attr_once(const void *kern, int64_t smem, int cluster);
+int occupancy_cached(const void *kern, int threads, int64_t smem, int cluster, int *per_sm_or_clusters);
+
 // ------------------------------------------------------------- launchers --
 struct LaunchStats {
   int launches = 0;

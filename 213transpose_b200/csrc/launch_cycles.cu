@@ -264,14 +264,13 @@ int launch_seg_cycles(const CycleTable &ct, char *data, int64_t d3, int64_t slic
       return with_perm<U>(ct.spec, [&](auto dst) -> bool {
         using P = decltype(dst);
         auto kern = k_seg_cycles_bulk<P, U>;
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) {
-          status = cuda_status(e, "cudaFuncSetAttribute(bulk walker)");
+        if (!kernel_attr_once((const void *)kern, smem, 1)) {
+          status = cuda_status(cudaGetLastError(), "cudaFuncSetAttribute(bulk walker)");
           return true;
         }
-        int per_sm = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32, (size_t)smem) != cudaSuccess || per_sm < 1)
-          per_sm = 1;
+        int per_sm = 1;
+        occupancy_cached((const void *)kern, 32, smem, 1, &per_sm);
+        cudaError_t e;
         const int64_t items = ct.n_chunks * npieces * d3;
         const int64_t grid = std::max<int64_t>(1, std::min<int64_t>((int64_t)per_sm * d.sms, items));
         kern<<<(unsigned)grid, 32, (size_t)smem, st>>>(data, slice_bytes, d3, seg_bytes, piece, npieces,

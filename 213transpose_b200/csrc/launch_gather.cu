@@ -163,12 +163,7 @@ RowCfg row_config(int64_t m, int64_t n, int eb, const void *data) {
 
 template <typename Kern>
 int prep_kernel(Kern kern, int64_t smem, int K) {
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(smem)");
-  if (K > 8) {
-    e = cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(cluster)");
-  }
+  if (!kernel_attr_once((const void *)kern, smem, K)) return cuda_status(cudaGetLastError(), "cudaFuncSetAttribute");
   return T213_OK;
 }
 
@@ -176,32 +171,10 @@ int prep_kernel(Kern kern, int64_t smem, int K) {
 template <typename Kern>
 int64_t persistent_grid(Kern kern, int threads, int64_t smem, int K, int64_t units) {
   const DevInfo &d = dev_info();
-  if (K <= 1) {
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, (size_t)smem) != cudaSuccess ||
-        per_sm < 1)
-      per_sm = 1;
-    int64_t g = (int64_t)per_sm * d.sms;
-    return std::max<int64_t>(1, std::min<int64_t>(g, units));
-  }
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3((unsigned)(K * 8), 1, 1);
-  cfg.blockDim = dim3(threads, 1, 1);
-  cfg.dynamicSmemBytes = (size_t)smem;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = K;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  int clusters = 0;
-  if (cudaOccupancyMaxActiveClusters(&clusters, kern, &cfg) != cudaSuccess || clusters < 1) {
-    cudaGetLastError();
-    clusters = std::max(1, d.sms / K);
-  }
-  int64_t c = std::min<int64_t>(clusters, units);
-  return std::max<int64_t>(1, c) * K;
+  int v = 1;
+  occupancy_cached((const void *)kern, threads, smem, K, &v);
+  if (K <= 1) return std::max<int64_t>(1, std::min<int64_t>((int64_t)v * d.sms, units));
+  return std::max<int64_t>(1, std::min<int64_t>(v, units)) * K;
 }
 
 template <typename Kern, typename... Args>

@@ -11,9 +11,8 @@ namespace {
 template <typename Kern>
 int64_t resident_grid(Kern kern, int threads, size_t smem, int64_t units) {
   const DevInfo &d = dev_info();
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1)
-    per_sm = 1;
+  int per_sm = 1;
+  occupancy_cached((const void *)kern, threads, (int64_t)smem, 1, &per_sm);
   return std::max<int64_t>(1, std::min<int64_t>((int64_t)per_sm * d.sms, units));
 }
 
@@ -116,8 +115,8 @@ int launch_band_transpose(char *data, int64_t n_bands, int64_t R, int64_t C, int
       constexpr int EB = decltype(EBc)::value;
       constexpr bool VEC = decltype(VECc)::value;
       auto kern = k_band_bulk<EB, VEC>;
-      cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(band bulk)");
+      if (!kernel_attr_once((const void *)kern, smem, 1)) return cuda_status(cudaGetLastError(), "cudaFuncSetAttribute(band bulk)");
+      cudaError_t e;
       const int64_t grid = resident_grid(kern, kTileThreads, (size_t)smem, n_bands);
       const uint32_t cq = (uint32_t)std::max<int64_t>(1, C / (16 / EB));
       kern<<<(unsigned)grid, kTileThreads, (size_t)smem, st>>>(data, n_bands, (uint32_t)R, (uint32_t)C, nbuf,
@@ -147,8 +146,8 @@ int launch_band_transpose(char *data, int64_t n_bands, int64_t R, int64_t C, int
   auto go = [&](auto EBc) -> int {
     constexpr int EB = decltype(EBc)::value;
     auto kern = k_band_transpose<EB>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_status(e, "cudaFuncSetAttribute(band)");
+    if (!kernel_attr_once((const void *)kern, smem, 1)) return cuda_status(cudaGetLastError(), "cudaFuncSetAttribute(band)");
+    cudaError_t e;
     const int64_t grid = resident_grid(kern, kTileThreads, (size_t)smem, n_bands);
     kern<<<(unsigned)grid, kTileThreads, (size_t)smem, st>>>(data, n_bands, (uint32_t)R, (uint32_t)C, S,
                                                             FastDiv<uint32_t>((uint64_t)C),

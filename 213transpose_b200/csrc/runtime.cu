@@ -8,6 +8,7 @@
 #include <cstring>
 #include <list>
 #include <map>
+#include <tuple>
 
 #include "plan.h"
 
@@ -106,6 +107,74 @@ static void release_workspaces() {
       ++it;
     }
   }
+}
+
+// ----------------------------------------------------------- launch cache --
+namespace {
+std::mutex g_lc_mu;
+std::map<std::tuple<const void *, int64_t, int, int>, int> g_attr_done;
+std::map<std::tuple<const void *, int, int64_t, int, int>, int> g_occ;
+}  // namespace
+
+bool kernel_attr_once(const void *kern, int64_t smem, int cluster) {
+  // The dynamic shared-memory attribute is an upper bound: raise it when a
+  // launch needs more than any earlier one, never lower it.
+  const int dev = dev_info().id;
+  std::lock_guard<std::mutex> lk(g_lc_mu);
+  auto key = std::make_tuple(kern, (int64_t)0, 0, dev);
+  auto it = g_attr_done.find(key);
+  const int64_t have = it == g_attr_done.end() ? -1 : it->second;
+  if (smem > have) {
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return false;
+    g_attr_done[key] = (int)smem;
+  }
+  if (cluster > 8) {
+    auto ck = std::make_tuple(kern, (int64_t)1, 1, dev);
+    if (!g_attr_done.count(ck)) {
+      if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) return false;
+      g_attr_done[ck] = 1;
+    }
+  }
+  return true;
+}
+
+int occupancy_cached(const void *kern, int threads, int64_t smem, int cluster, int *out) {
+  const int dev = dev_info().id;
+  {
+    std::lock_guard<std::mutex> lk(g_lc_mu);
+    auto it = g_occ.find(std::make_tuple(kern, threads, smem, cluster, dev));
+    if (it != g_occ.end()) {
+      *out = it->second;
+      return T213_OK;
+    }
+  }
+  int v = 0;
+  if (cluster <= 1) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kern, threads, (size_t)smem) != cudaSuccess || v < 1) {
+      cudaGetLastError();
+      v = 1;
+    }
+  } else {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(cluster * 8), 1, 1);
+    cfg.blockDim = dim3(threads, 1, 1);
+    cfg.dynamicSmemBytes = (size_t)smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (cudaOccupancyMaxActiveClusters(&v, kern, &cfg) != cudaSuccess || v < 1) {
+      cudaGetLastError();
+      v = std::max(1, dev_info().sms / cluster);
+    }
+  }
+  std::lock_guard<std::mutex> lk(g_lc_mu);
+  g_occ[std::make_tuple(kern, threads, smem, cluster, dev)] = v;
+  *out = v;
+  return T213_OK;
 }
 
 // ------------------------------------------------------------------ timing --
@@ -211,14 +280,16 @@ int add_seg_pass(Plan &P, const PermSpec &ps, int64_t seg_bytes, bool skip_ident
   return T213_OK;
 }
 
+// Fraction of the copy bandwidth a segment-cycle pass reaches, by segment
+// size (bulk-copy walker from 1 KB up, register walker below).
 double seg_eff(int64_t seg_bytes) {
-  if (seg_bytes >= 2048) return 0.9;
-  if (seg_bytes >= 1024) return 0.85;
-  if (seg_bytes >= 512) return 0.75;
-  if (seg_bytes >= 256) return 0.6;
-  if (seg_bytes >= 128) return 0.5;
-  if (seg_bytes >= 64) return 0.3;
-  return 0.12;
+  if (seg_bytes >= 4096) return 0.88;
+  if (seg_bytes >= 1024) return 0.8;
+  if (seg_bytes >= 512) return 0.55;
+  if (seg_bytes >= 256) return 0.4;
+  if (seg_bytes >= 128) return 0.3;
+  if (seg_bytes >= 64) return 0.18;
+  return 0.08;
 }
 
 std::string fmt_plan(const Plan &P) {
@@ -298,14 +369,14 @@ void r2c_passes(Plan &P, int64_t m, int64_t n, bool skinny) {
 double gather_cost(const PassDesc &p, int eb) {
   if (p.type == PT_COL) {
     std::string d = describe_col_gather(p.m, p.n, eb, nullptr);
-    if (d.find("scratch") != std::string::npos) return 1 / 0.3;
-    if (d.find("cluster=1 ") != std::string::npos) return 1 / 0.8;
-    return 1 / 0.7;
+    if (d.find("scratch") != std::string::npos) return 1 / 0.2;
+    if (d.find("cluster=1 ") != std::string::npos) return 1 / 0.45;
+    return 1 / 0.3;
   }
   std::string d = describe_row_gather(p.m, p.n, eb, nullptr);
-  if (d.find("scratch") != std::string::npos) return 1 / 0.35;
-  if (d.find("cluster") != std::string::npos) return 1 / 0.75;
-  return 1 / 0.85;
+  if (d.find("scratch") != std::string::npos) return 1 / 0.25;
+  if (d.find("cluster") != std::string::npos) return 1 / 0.45;
+  return 1 / 0.65;
 }
 
 int64_t largest_divisor_le(int64_t x, int64_t limit) {
@@ -322,7 +393,8 @@ int64_t largest_divisor_le(int64_t x, int64_t limit) {
 // Candidate block / band sizes.
 int64_t pick_block_t(int64_t m, int64_t n) { return ext_gcd(m, n, nullptr); }
 int64_t pick_band_t(int64_t m, int64_t n, int eb) {
-  // t | m, band t x n fits shared memory
+  // t | m, band t x n fits shared memory; a whole slice up to 96 KB is one band
+  if (band_smem_bytes(m, n, eb) <= 96 * 1024) return m;
   int64_t per_row = band_smem_bytes(1, n, eb);
   if (per_row > band_smem_limit()) return 0;
   return largest_divisor_le(m, band_smem_limit() / per_row);
@@ -449,10 +521,10 @@ double plan_cost(const Plan &P) {
         break;
       }
       case PT_TILE:
-        c += 1 / 0.9;
+        c += (p.t % 32 == 0 && P.eb >= 4) ? 1 / 0.75 : 1 / 0.35;
         break;
       case PT_BAND:
-        c += 1 / 0.85;
+        c += 1 / 0.5;
         break;
     }
   }
@@ -466,18 +538,19 @@ double estimate_cost(int kind, int64_t m, int64_t n, int64_t t, int eb, int64_t 
   switch (kind) {
     case T213_PLAN_BLOCKS: {
       if (t <= 0 || t * eb < 16) return 1e9;
-      if (m == n && m == t) return 1 / 0.9;
+      const double tile = (t % 32 == 0 && eb >= 4) ? 1 / 0.75 : 1 / 0.35;
+      if (m == n && m == t) return tile;
       double S = (double)m * (double)n / (double)t;
       if (S > S_limit) return 1e9;
-      return 1 / 0.9 + 1 / seg_eff(t * eb);
+      return tile + 1 / seg_eff(t * eb);
     }
     case T213_PLAN_BANDS:
     case T213_PLAN_BANDS_T: {
       if (t <= 0 || t * eb < 32) return 1e9;
       double S = (double)m * (double)n / (double)t;
       if (S > S_limit) return 1e9;
-      if ((kind == T213_PLAN_BANDS && t == m) || (kind == T213_PLAN_BANDS_T && t == n)) return 1 / 0.85;
-      return 1 / 0.85 + 1 / seg_eff(t * eb);
+      if ((kind == T213_PLAN_BANDS && t == m) || (kind == T213_PLAN_BANDS_T && t == n)) return 1 / 0.5;
+      return 1 / 0.5 + 1 / seg_eff(t * eb);
     }
   }
   return 1e9;

@@ -35,12 +35,19 @@ ClassKey class_of(int64_t d1, int64_t d2, int64_t d3, int eb) {
 }
 
 std::mutex g_mu;
-std::map<ClassKey, int> g_cache;
+std::map<ClassKey, int> g_cache;                                     // per shape class
+std::map<std::tuple<int64_t, int64_t, int64_t, int>, int> g_exact;  // per exact shape, wins
 
 }  // namespace
 
 int tuner_lookup_internal(int64_t d1, int64_t d2, int64_t d3, int eb, int *kind, int64_t *t) {
   std::lock_guard<std::mutex> lk(g_mu);
+  auto ex = g_exact.find(std::make_tuple(d1, d2, d3, eb));
+  if (ex != g_exact.end()) {
+    *kind = ex->second;
+    *t = 0;
+    return T213_OK;
+  }
   auto it = g_cache.find(class_of(d1, d2, d3, eb));
   if (it == g_cache.end()) return T213_ERR_NOT_READY;
   *kind = it->second;
@@ -65,6 +72,7 @@ int t213_tuner_lookup(int64_t d1, int64_t d2, int64_t d3, int32_t elem_bytes, in
 int t213_tuner_clear(void) {
   std::lock_guard<std::mutex> lk(g_mu);
   g_cache.clear();
+  g_exact.clear();
   return T213_OK;
 }
 
@@ -76,9 +84,14 @@ int t213_tuner_save(const char *path) {
     return T213_ERR_INVALID_ARGUMENT;
   }
   std::lock_guard<std::mutex> lk(g_mu);
-  fprintf(f, "# t213 tuner cache: eb log2(d1) log2(d2) log2(d3) log2(gcd) plan_kind\n");
+  fprintf(f, "# t213 tuner cache\n# class eb log2(d1) log2(d2) log2(d3) log2(gcd) plan_kind\n");
+  fprintf(f, "# shape d1 d2 d3 eb plan_kind\n");
   for (auto &kv : g_cache)
-    fprintf(f, "%d %d %d %d %d %d\n", kv.first.eb, kv.first.l1, kv.first.l2, kv.first.l3, kv.first.lg, kv.second);
+    fprintf(f, "class %d %d %d %d %d %d\n", kv.first.eb, kv.first.l1, kv.first.l2, kv.first.l3, kv.first.lg,
+            kv.second);
+  for (auto &kv : g_exact)
+    fprintf(f, "shape %lld %lld %lld %d %d\n", (long long)std::get<0>(kv.first), (long long)std::get<1>(kv.first),
+            (long long)std::get<2>(kv.first), std::get<3>(kv.first), kv.second);
   fclose(f);
   return T213_OK;
 }
@@ -96,10 +109,15 @@ int t213_tuner_load(const char *path) {
   while (fgets(line, sizeof line, f)) {
     if (line[0] == '#') continue;
     ClassKey k;
-    int kind;
-    if (sscanf(line, "%d %d %d %d %d %d", &k.eb, &k.l1, &k.l2, &k.l3, &k.lg, &kind) == 6 && kind >= T213_PLAN_AUTO &&
-        kind <= T213_PLAN_IDENTITY) {
+    int kind, eb;
+    long long a, b, c;
+    if (sscanf(line, "class %d %d %d %d %d %d", &k.eb, &k.l1, &k.l2, &k.l3, &k.lg, &kind) == 6 &&
+        kind >= T213_PLAN_AUTO && kind <= T213_PLAN_IDENTITY) {
       g_cache[k] = kind;
+      n++;
+    } else if (sscanf(line, "shape %lld %lld %lld %d %d", &a, &b, &c, &eb, &kind) == 5 && kind >= T213_PLAN_AUTO &&
+               kind <= T213_PLAN_IDENTITY) {
+      g_exact[std::make_tuple((int64_t)a, (int64_t)b, (int64_t)c, eb)] = kind;
       n++;
     }
   }
@@ -155,6 +173,7 @@ int t213_tune_shape(void *scratch_data, int64_t d1, int64_t d2, int64_t d3, int3
   {
     std::lock_guard<std::mutex> lk(g_mu);
     g_cache[class_of(d1, d2, d3, elem_bytes)] = best_kind;
+    g_exact[std::make_tuple(d1, d2, d3, (int)elem_bytes)] = best_kind;
   }
   if (chosen_plan) *chosen_plan = best_kind;
   if (chosen_t) *chosen_t = best_t;

@@ -198,6 +198,11 @@ int t213_batch_execute(t213_batch batch, t213_stream_t stream);
 int t213_batch_status(t213_batch batch, t213_stream_t stream);
 int t213_batch_describe(t213_batch batch, char *buf, size_t buflen);
 int t213_batch_destroy(t213_batch batch);
+/* Autotunes every shape class present in the list (timing the applicable
+ * plan families on scratch memory of the class's largest tensor) so that
+ * t213_batch_create and the plain call pick the measured winner.
+ * Synchronous; the tensors' data are not touched. */
+int t213_batch_tune(const t213_tensor_desc *tensors, int32_t count, t213_stream_t stream);
 /* Baseline form: the plain call looped over the same list on one stream. */
 int t213_transpose_looped(const t213_tensor_desc *tensors, int32_t count, t213_stream_t stream);
 

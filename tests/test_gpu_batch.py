@@ -1,0 +1,90 @@
+"""The batched form: one persistent, graph-captured launch over many uneven
+tensors gives, for every tensor, the same bytes as the oracle and as the
+looped plain call."""
+import importlib
+import random
+
+import numpy as np
+import pytest
+
+from conftest import from_device, to_device
+
+pytestmark = pytest.mark.gpu
+
+
+def _mixed_shapes(seed):
+    rng = random.Random(seed)
+    out = []
+    plans = ["auto", "c2r", "r2c", "blocks", "bands", "bands_t", "skinny"]
+    for i in range(48):
+        d1, d2 = rng.randint(1, 700), rng.randint(1, 700)
+        if i % 5 == 0:  # gcd-rich shapes for block plans
+            g = rng.choice([32, 64, 96, 128])
+            d1, d2 = g * rng.randint(1, 6), g * rng.randint(1, 6)
+        if i % 7 == 0:  # skinny
+            d2 = rng.randint(1, 32)
+        d3 = rng.randint(1, 3)
+        eb = rng.choice([4, 8, 16, 4, 1, 2])
+        out.append((d1, d2, d3, eb, plans[i % len(plans)]))
+    return out
+
+
+def _applicable(t213, d1, d2, d3, eb, plan):
+    try:
+        t213.describe(d1, d2, d3, eb, plan)
+        return plan
+    except t213.T213Error:
+        return "auto"
+
+
+def test_batch_matches_oracle_and_loop(cuda, oracle, t213):
+    shapes = [(d1, d2, d3, eb, _applicable(t213, d1, d2, d3, eb, p)) for d1, d2, d3, eb, p in _mixed_shapes(11)]
+    hosts, wants, devs = [], [], []
+    for i, (d1, d2, d3, eb, _) in enumerate(shapes):
+        x = oracle.random_bits(d1 * d2 * d3, eb, 100 + i)
+        hosts.append(x)
+        wants.append(oracle.gather213(x.view(np.dtype((np.void, eb))), d1, d2, d3).view(np.uint8))
+        devs.append(to_device(cuda, x))
+    B = t213.Batch([(dev, d1, d2, d3, eb, plan) for dev, (d1, d2, d3, eb, plan) in zip(devs, shapes)])
+    assert "batch: 48 tensors" in B.describe()
+    for rep in range(2):  # first call captures the graph, the second replays it
+        for dev, x in zip(devs, hosts):
+            dev.copy_(cuda.from_numpy(x))
+        B.execute()
+        assert B.status() == 0
+        for i, (dev, want) in enumerate(zip(devs, wants)):
+            assert np.array_equal(from_device(dev), want), (rep, shapes[i])
+    for dev, x in zip(devs, hosts):
+        dev.copy_(cuda.from_numpy(x))
+    B.looped()
+    cuda.cuda.synchronize()
+    for i, (dev, want) in enumerate(zip(devs, wants)):
+        assert np.array_equal(from_device(dev), want), ("looped", shapes[i])
+    B.close()
+
+
+def test_batch_full_config_round_trip(cuda, t213):
+    """All 512 tensors of the batched configuration (seed 1): one batch, then a
+    second batch with the axes swapped restores every tensor bit for bit."""
+    w = importlib.import_module("213transpose_b200.workloads")
+    shapes = w.batched_shapes(1, 512)
+    gen = cuda.Generator(device="cuda").manual_seed(1)
+    devs, origs = [], []
+    for d1, d2, d3, eb, _ in shapes:
+        x = cuda.empty(d1 * d2 * d3 * eb, dtype=cuda.uint8, device="cuda")
+        x.random_(0, 256, generator=gen)
+        devs.append(x)
+        origs.append(x.clone())
+    fwd = t213.Batch([(x, d1, d2, d3, eb) for x, (d1, d2, d3, eb, _) in zip(devs, shapes)])
+    back = t213.Batch([(x, d2, d1, d3, eb) for x, (d1, d2, d3, eb, _) in zip(devs, shapes)])
+    fwd.execute()
+    assert fwd.status() == 0
+    # spot-check a few tensors of the forward batch against torch's permute
+    for i in range(0, 512, 97):
+        d1, d2, d3, eb, _ = shapes[i]
+        want = origs[i].view(d3, d2, d1, eb).permute(0, 2, 1, 3).contiguous().view(-1)
+        assert cuda.equal(devs[i], want), shapes[i]
+    back.execute()
+    assert back.status() == 0
+    bad = [shapes[i] for i in range(512) if not cuda.equal(devs[i], origs[i])]
+    assert not bad, bad[:5]
