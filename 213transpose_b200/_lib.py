@@ -42,6 +42,11 @@ class TensorDesc(ctypes.Structure):
                 ("elem_bytes", ctypes.c_int32), ("plan_kind", ctypes.c_int32)]
 
 
+class Request(ctypes.Structure):
+    _fields_ = [("d1", ctypes.c_int64), ("d2", ctypes.c_int64), ("d3", ctypes.c_int64), ("elem_bytes", ctypes.c_int32),
+                ("plan_kind", ctypes.c_int32), ("arrival_s", ctypes.c_double), ("seed", ctypes.c_uint64)]
+
+
 class ServeStats(ctypes.Structure):
     _fields_ = [("completed", ctypes.c_int64), ("rejected", ctypes.c_int64), ("bytes_done", ctypes.c_int64),
                 ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
@@ -87,6 +92,12 @@ _SIGS = {
     "t213_tuner_save": ([ctypes.c_char_p], ctypes.c_int),
     "t213_tuner_clear": ([], ctypes.c_int),
     "t213_tuner_lookup": ([_i64, _i64, _i64, _i32, ctypes.POINTER(_i32), _pi64], ctypes.c_int),
+    "t213_server_create": ([_i64, _i32, _i32, ctypes.POINTER(_vp)], ctypes.c_int),
+    "t213_server_run": ([_vp, ctypes.POINTER(Request), _i32, ctypes.POINTER(ServeStats),
+                         ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+    "t213_server_expected_checksum": ([_vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+    "t213_server_run_alone": ([_vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
+    "t213_server_destroy": ([_vp], ctypes.c_int),
 }
 
 

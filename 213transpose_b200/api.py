@@ -257,6 +257,60 @@ class Batch:
             pass
 
 
+class Server:
+    """The serving form (include/t213_serve.h): HBM-budget admission into a
+    device arena, continuous dispatch onto a stream pool, p50/p99 latency."""
+
+    def __init__(self, hbm_budget_bytes=150 * 10**9, max_inflight=64, streams=8):
+        h = ctypes.c_void_p(0)
+        check(lib().t213_server_create(int(hbm_budget_bytes), int(max_inflight), int(streams), ctypes.byref(h)))
+        self._h = h
+
+    @staticmethod
+    def _requests(reqs):
+        arr = (_lib.Request * max(1, len(reqs)))()
+        for i, r in enumerate(reqs):
+            kind = r.get("plan", "auto")
+            kind = _lib.PLAN_NAMES[kind] if isinstance(kind, str) else int(kind)
+            arr[i] = _lib.Request(int(r["d1"]), int(r["d2"]), int(r["d3"]), int(r["elem_bytes"]), kind,
+                                  float(r.get("t", r.get("arrival_s", 0.0))), int(r.get("seed", i + 1)))
+        return arr
+
+    def run(self, reqs):
+        """Replays the schedule; returns (stats dict, checksums, latencies_ms)."""
+        n = len(reqs)
+        arr = self._requests(reqs)
+        st = _lib.ServeStats()
+        sums = (ctypes.c_uint64 * max(1, n))()
+        lat = (ctypes.c_double * max(1, n))()
+        check(lib().t213_server_run(self._h, arr, n, ctypes.byref(st), sums, lat))
+        stats = {f: getattr(st, f) for f, _ in _lib.ServeStats._fields_}
+        return stats, list(sums)[:n], list(lat)[:n]
+
+    def expected_checksum(self, req) -> int:
+        arr = self._requests([req])
+        v = ctypes.c_uint64(0)
+        check(lib().t213_server_expected_checksum(self._h, arr, ctypes.byref(v)))
+        return int(v.value)
+
+    def run_alone(self, req) -> int:
+        arr = self._requests([req])
+        v = ctypes.c_uint64(0)
+        check(lib().t213_server_run_alone(self._h, arr, ctypes.byref(v)))
+        return int(v.value)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().t213_server_destroy(self._h)
+            self._h = ctypes.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def _stream_of(stream):
     if stream is None:
         torch = _t()

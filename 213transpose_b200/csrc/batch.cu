@@ -551,6 +551,7 @@ int t213_batch_describe(t213_batch B, char *buf, size_t buflen) {
 
 int t213_batch_destroy(t213_batch B) {
   if (!B) return T213_OK;
+  cudaDeviceSynchronize();  // an execute may still be running; cudaFree does not wait for it
   if (B->exec) cudaGraphExecDestroy(B->exec);
   if (B->graph) cudaGraphDestroy(B->graph);
   if (B->d_passes) cudaFree(B->d_passes);

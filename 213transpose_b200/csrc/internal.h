@@ -40,6 +40,15 @@ int *device_status_word(int *status);
 // Grow-only scratch buffer per (device, stream).  Calls on one stream run in
 // order, so they can share it; calls on different streams never do.
 char *workspace(cudaStream_t st, size_t bytes, int *status);
+// Frees the workspace of one stream (before the stream is destroyed).
+void release_stream_workspace(cudaStream_t st);
+
+// Device memory that kernels in flight on any stream may still read (cycle
+// tables of evicted plans) is not freed at once: cudaFree does not promise to
+// wait for them.  It is parked here and freed after a device-wide
+// synchronisation, once enough has accumulated or on t213_release_cache.
+void defer_free(int dev, void *p);
+void flush_deferred_frees();
 
 // ------------------------------------------------------------- functors --
 struct FnSpec {

@@ -16,13 +16,44 @@
 namespace t213 {
 
 CycleTable::~CycleTable() {
-  if (!d_chunks && !d_carry_items) return;
+  if (d_chunks) defer_free(dev, d_chunks);
+  if (d_carry_items) defer_free(dev, d_carry_items);
+}
+
+namespace {
+std::mutex g_grave_mu;
+std::vector<std::pair<int, void *>> g_grave;
+constexpr size_t kGraveMax = 256;
+
+void flush_locked() {
+  if (g_grave.empty()) return;
   int cur = 0;
   cudaGetDevice(&cur);
-  if (cur != dev) cudaSetDevice(dev);
-  if (d_chunks) cudaFree(d_chunks);
-  if (d_carry_items) cudaFree(d_carry_items);
-  if (cur != dev) cudaSetDevice(cur);
+  std::vector<int> devs;
+  for (auto &e : g_grave)
+    if (std::find(devs.begin(), devs.end(), e.first) == devs.end()) devs.push_back(e.first);
+  for (int d : devs) {
+    cudaSetDevice(d);
+    cudaDeviceSynchronize();  // nothing in flight can still read the tables
+  }
+  for (auto &e : g_grave) {
+    cudaSetDevice(e.first);
+    cudaFree(e.second);
+  }
+  g_grave.clear();
+  cudaSetDevice(cur);
+}
+}  // namespace
+
+void defer_free(int dev, void *p) {
+  std::lock_guard<std::mutex> lk(g_grave_mu);
+  g_grave.push_back({dev, p});
+  if (g_grave.size() > kGraveMax) flush_locked();
+}
+
+void flush_deferred_frees() {
+  std::lock_guard<std::mutex> lk(g_grave_mu);
+  flush_locked();
 }
 
 namespace {
@@ -127,7 +158,7 @@ struct Key {
 
 std::mutex g_mu;
 std::list<std::pair<Key, std::shared_ptr<CycleTable>>> g_cache;  // front = most recent
-constexpr size_t kCacheMax = 64;
+constexpr size_t kCacheMax = 256;
 
 }  // namespace
 

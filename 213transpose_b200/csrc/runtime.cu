@@ -61,7 +61,10 @@ char *workspace(cudaStream_t st, size_t bytes, int *status) {
   auto &w = g_ws[{dev, st}];
   if (w.first && w.second >= bytes) return w.first;
   if (w.first) {
-    cudaFree(w.first);  // waits for work that may still use it
+    // cudaFree does not promise to wait for kernels in flight: finish the
+    // stream's earlier work (the only user of this buffer) first
+    cudaStreamSynchronize(st);
+    cudaFree(w.first);
     w.first = nullptr;
     w.second = 0;
   }
@@ -94,6 +97,16 @@ int *device_status_word(int *status) {
   }
   words[dev] = p;
   return p;
+}
+
+void release_stream_workspace(cudaStream_t st) {
+  const int dev = dev_info().id;
+  std::lock_guard<std::mutex> lk(g_ws_mu);
+  auto it = g_ws.find({dev, st});
+  if (it == g_ws.end()) return;
+  cudaStreamSynchronize(st);
+  if (it->second.first) cudaFree(it->second.first);
+  g_ws.erase(it);
 }
 
 static void release_workspaces() {
@@ -305,10 +318,10 @@ std::string fmt_plan(const Plan &P) {
     s += " ";
     switch (p.type) {
       case PT_COL:
-        snprintf(buf, sizeof buf, "col_gather(fn=%d)", p.fn.kind);
+        snprintf(buf, sizeof buf, "col_gather(fn=%d)%s", p.fn.kind, describe_col_gather(p.m, p.n, P.eb, nullptr).substr(10).c_str());
         break;
       case PT_ROW:
-        snprintf(buf, sizeof buf, "row_gather(fn=%d)", p.fn.kind);
+        snprintf(buf, sizeof buf, "row_gather(fn=%d)%s", p.fn.kind, describe_row_gather(p.m, p.n, P.eb, nullptr).substr(10).c_str());
         break;
       case PT_SEG:
         snprintf(buf, sizeof buf, "segment_cycles(S=%lld seg=%lldB cycles=%lld chunks=%lld carry=%lld maxlen=%lld)",
@@ -534,7 +547,7 @@ double plan_cost(const Plan &P) {
 // Cheap estimate used to rank candidates before any cycle table is built.
 double estimate_cost(int kind, int64_t m, int64_t n, int64_t t, int eb, int64_t d3) {
   (void)d3;
-  const double S_limit = 6.0e7;  // host cycle walk stays below ~0.3 s
+  const double S_limit = 4.0e6;  // first-call host cycle walk stays around 20 ms
   switch (kind) {
     case T213_PLAN_BLOCKS: {
       if (t <= 0 || t * eb < 16) return 1e9;
@@ -566,8 +579,13 @@ struct PlanKey {
   }
 };
 
+// LRU cache of plans (front = most recently used).  Evicting a plan can drop
+// the last reference to its cycle tables; their device memory is then freed
+// only after a device-wide synchronisation (see CycleTable).
 std::mutex g_plan_mu;
-std::map<PlanKey, std::shared_ptr<Plan>> g_plans;
+std::list<std::pair<PlanKey, std::shared_ptr<Plan>>> g_plan_lru;
+std::map<PlanKey, std::list<std::pair<PlanKey, std::shared_ptr<Plan>>>::iterator> g_plans;
+constexpr size_t kPlanCacheMax = 1024;
 
 std::shared_ptr<Plan> new_plan(int64_t d1, int64_t d2, int64_t d3, int eb) {
   auto P = std::make_shared<Plan>();
@@ -597,7 +615,10 @@ std::shared_ptr<Plan> get_plan(int64_t d1, int64_t d2, int64_t d3, int eb, int k
   {
     std::lock_guard<std::mutex> lk(g_plan_mu);
     auto it = g_plans.find(key);
-    if (it != g_plans.end()) return it->second;
+    if (it != g_plans.end()) {
+      g_plan_lru.splice(g_plan_lru.begin(), g_plan_lru, it->second);
+      return it->second->second;
+    }
   }
   std::shared_ptr<Plan> best;
   if (kind != T213_PLAN_AUTO) {
@@ -659,8 +680,15 @@ std::shared_ptr<Plan> get_plan(int64_t d1, int64_t d2, int64_t d3, int eb, int k
   best->desc = fmt_plan(*best);
   {
     std::lock_guard<std::mutex> lk(g_plan_mu);
-    g_plans[key] = best;
-    if (g_plans.size() > 256) g_plans.erase(g_plans.begin());
+    auto it = g_plans.find(key);
+    if (it == g_plans.end()) {
+      g_plan_lru.push_front({key, best});
+      g_plans[key] = g_plan_lru.begin();
+      while (g_plan_lru.size() > kPlanCacheMax) {
+        g_plans.erase(g_plan_lru.back().first);
+        g_plan_lru.pop_back();
+      }
+    }
   }
   return best;
 }
@@ -1085,8 +1113,10 @@ int t213_release_cache(void) {
   {
     std::lock_guard<std::mutex> lk(g_plan_mu);
     g_plans.clear();
+    g_plan_lru.clear();
   }
   release_workspaces();
+  flush_deferred_frees();
   return T213_OK;
 }
 

@@ -1,0 +1,414 @@
+// Serving runtime (include/t213_serve.h): HBM-budget admission into a device
+// arena, continuous dispatch of admitted requests onto a stream pool,
+// completion polling and latency statistics.
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <thread>
+#include <vector>
+
+#include "../../include/t213_serve.h"
+#include "plan.h"
+
+namespace t213 {
+namespace {
+
+// splitmix64 finaliser (Vigna): the fill and the checksums are built on it.
+__host__ __device__ __forceinline__ uint64_t smix(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+// Word w (0 or 1) of element e of a request's tensor.
+__device__ __forceinline__ uint64_t fill_word(uint64_t seed, uint64_t e, int w) {
+  return smix(seed * 0xD1B54A32D192ED03ull ^ (e * 2 + (uint64_t)w));
+}
+
+// An element folded to 64 bits (the first eb bytes of its words).
+__device__ __forceinline__ uint64_t fold(uint64_t w0, uint64_t w1, int eb) {
+  if (eb >= 16) return w0 ^ ((w1 << 17) | (w1 >> 47));
+  if (eb == 8) return w0;
+  return w0 & ((1ull << (8 * eb)) - 1);
+}
+
+__device__ __forceinline__ uint64_t term(uint64_t pos, uint64_t v) { return smix(pos * 0x100000001B3ull ^ v); }
+
+__global__ void k_fill(unsigned char *p, int64_t nel, int eb, uint64_t seed) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t w0 = fill_word(seed, (uint64_t)e, 0);
+    switch (eb) {
+      case 1:
+        p[e] = (unsigned char)w0;
+        break;
+      case 2:
+        reinterpret_cast<uint16_t *>(p)[e] = (uint16_t)w0;
+        break;
+      case 4:
+        reinterpret_cast<uint32_t *>(p)[e] = (uint32_t)w0;
+        break;
+      case 8:
+        reinterpret_cast<unsigned long long *>(p)[e] = w0;
+        break;
+      default: {
+        const uint64_t w1 = fill_word(seed, (uint64_t)e, 1);
+        reinterpret_cast<uint4 *>(p)[e] = make_uint4((uint32_t)w0, (uint32_t)(w0 >> 32), (uint32_t)w1, (uint32_t)(w1 >> 32));
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void reduce_add(uint64_t v, unsigned long long *out) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, (unsigned long long)v);
+}
+
+__global__ void k_checksum(const unsigned char *p, int64_t nel, int eb, unsigned long long *out) {
+  uint64_t acc = 0;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t w0 = 0, w1 = 0;
+    switch (eb) {
+      case 1:
+        w0 = p[e];
+        break;
+      case 2:
+        w0 = reinterpret_cast<const uint16_t *>(p)[e];
+        break;
+      case 4:
+        w0 = reinterpret_cast<const uint32_t *>(p)[e];
+        break;
+      case 8:
+        w0 = reinterpret_cast<const unsigned long long *>(p)[e];
+        break;
+      default: {
+        const uint4 v = reinterpret_cast<const uint4 *>(p)[e];
+        w0 = (uint64_t)v.x | ((uint64_t)v.y << 32);
+        w1 = (uint64_t)v.z | ((uint64_t)v.w << 32);
+      }
+    }
+    acc += term((uint64_t)e, fold(w0, w1, eb));
+  }
+  reduce_add(acc, out);
+}
+
+// Checksum a correct 213 transpose must have: output position o holds the
+// element filled at source index src(o).
+__global__ void k_checksum_expected(int64_t d1, int64_t d2, int64_t d3, int eb, uint64_t seed,
+                                    unsigned long long *out) {
+  const int64_t nel = d1 * d2 * d3;
+  uint64_t acc = 0;
+  for (int64_t o = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; o < nel; o += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = o / (d1 * d2), r = o - k * d1 * d2;
+    const int64_t i1 = r / d2, i2 = r - i1 * d2;  // output is (d2 fastest, then d1)
+    const uint64_t src = (uint64_t)(k * d1 * d2 + i2 * d1 + i1);
+    uint64_t w0 = fill_word(seed, src, 0), w1 = eb >= 16 ? fill_word(seed, src, 1) : 0;
+    if (eb < 8) w0 &= (1ull << (8 * eb)) - 1;
+    acc += term((uint64_t)o, fold(w0, w1, eb));
+  }
+  reduce_add(acc, out);
+}
+
+// First-fit allocator over the device arena (host bookkeeping only).
+class Arena {
+ public:
+  void reset(int64_t bytes) {
+    free_.clear();
+    if (bytes > 0) free_[0] = bytes;
+    used_ = 0;
+  }
+  int64_t alloc(int64_t bytes) {
+    bytes = (bytes + 255) / 256 * 256;
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second >= bytes) {
+        const int64_t off = it->first, rest = it->second - bytes;
+        free_.erase(it);
+        if (rest > 0) free_[off + bytes] = rest;
+        used_ += bytes;
+        return off;
+      }
+    }
+    return -1;
+  }
+  void release(int64_t off, int64_t bytes) {
+    bytes = (bytes + 255) / 256 * 256;
+    used_ -= bytes;
+    auto it = free_.emplace(off, bytes).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+  int64_t used() const { return used_; }
+
+ private:
+  std::map<int64_t, int64_t> free_;
+  int64_t used_ = 0;
+};
+
+int grid_for(int64_t nel) {
+  const int64_t g = (nel + 255) / 256;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(g, (int64_t)dev_info().sms * 8));
+}
+
+}  // namespace
+}  // namespace t213
+
+using namespace t213;
+
+struct t213_server_st {
+  int dev = 0;
+  char *arena = nullptr;
+  int64_t arena_bytes = 0;
+  int max_inflight = 64;
+  std::vector<cudaStream_t> streams;
+  unsigned long long *d_sums = nullptr;
+  unsigned long long *h_sums = nullptr;  // pinned mirror
+  std::vector<cudaEvent_t> events;
+  Arena arena_map;
+};
+
+namespace {
+
+struct Slot {
+  int req = -1;
+  int64_t off = 0, bytes = 0;
+};
+
+int enqueue_request(t213_server s, const t213_request &r, int slot, int64_t off, cudaStream_t st) {
+  const int64_t nel = r.d1 * r.d2 * r.d3;
+  unsigned char *p = (unsigned char *)s->arena + off;
+  k_fill<<<grid_for(nel), 256, 0, st>>>(p, nel, r.elem_bytes, r.seed);
+  int rc = r.plan_kind == T213_PLAN_AUTO
+               ? t213_transpose(p, r.d1, r.d2, r.d3, r.elem_bytes, (t213_stream_t)st)
+               : t213_transpose_with_plan(p, r.d1, r.d2, r.d3, r.elem_bytes, r.plan_kind, 0, (t213_stream_t)st);
+  if (rc) return rc;
+  cudaMemsetAsync(s->d_sums + slot, 0, sizeof(unsigned long long), st);
+  k_checksum<<<grid_for(nel), 256, 0, st>>>(p, nel, r.elem_bytes, s->d_sums + slot);
+  cudaMemcpyAsync(s->h_sums + slot, s->d_sums + slot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaEventRecord(s->events[slot], st);
+  if (e != cudaSuccess) return cuda_status(e, "cudaEventRecord");
+  e = cudaGetLastError();
+  return e == cudaSuccess ? T213_OK : cuda_status(e, "request launch");
+}
+
+}  // namespace
+
+extern "C" {
+
+int t213_server_create(int64_t hbm_budget_bytes, int32_t max_inflight, int32_t n_streams, t213_server *out) {
+  if (!out || hbm_budget_bytes <= 0 || max_inflight <= 0 || n_streams <= 0) {
+    set_error("t213_server_create: bad arguments");
+    return T213_ERR_INVALID_ARGUMENT;
+  }
+  *out = nullptr;
+  auto *s = new t213_server_st();
+  s->dev = dev_info().id;
+  s->max_inflight = max_inflight;
+  size_t free_b = 0, total_b = 0;
+  cudaError_t e = cudaMemGetInfo(&free_b, &total_b);
+  if (e != cudaSuccess) {
+    delete s;
+    return cuda_status(e, "cudaMemGetInfo");
+  }
+  const int64_t margin = (int64_t)2 << 30;
+  s->arena_bytes = std::min<int64_t>(hbm_budget_bytes, (int64_t)free_b - margin);
+  if (s->arena_bytes <= 0) {
+    delete s;
+    set_error("not enough free device memory for the arena");
+    return T213_ERR_OUT_OF_MEMORY;
+  }
+  auto fail = [&](cudaError_t err, const char *w) {
+    int rc = cuda_status(err, w);
+    t213_server_destroy(s);
+    return rc;
+  };
+  if ((e = cudaMalloc(&s->arena, (size_t)s->arena_bytes))) return fail(e, "arena cudaMalloc");
+  s->arena_map.reset(s->arena_bytes);
+  if ((e = cudaMalloc(&s->d_sums, sizeof(unsigned long long) * max_inflight))) return fail(e, "sums");
+  if ((e = cudaMallocHost(&s->h_sums, sizeof(unsigned long long) * max_inflight))) return fail(e, "pinned sums");
+  for (int i = 0; i < n_streams; i++) {
+    cudaStream_t st;
+    if ((e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking))) return fail(e, "stream");
+    s->streams.push_back(st);
+    int rc = T213_OK;
+    if (!workspace(st, (size_t)64 << 20, &rc)) {  // carries of the cycle passes
+      t213_server_destroy(s);
+      return rc;
+    }
+  }
+  for (int i = 0; i < max_inflight; i++) {
+    cudaEvent_t ev;
+    if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming))) return fail(e, "event");
+    s->events.push_back(ev);
+  }
+  *out = s;
+  return T213_OK;
+}
+
+int t213_server_run(t213_server s, const t213_request *reqs, int32_t n, t213_serve_stats *stats, uint64_t *checksums,
+                    double *latency_ms) {
+  if (!s || n < 0 || (n > 0 && !reqs)) return T213_ERR_INVALID_ARGUMENT;
+  using clk = std::chrono::steady_clock;
+  std::vector<int> order(n);
+  for (int i = 0; i < n; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return reqs[a].arrival_s < reqs[b].arrival_s; });
+  std::vector<double> lat(n, -1.0);
+  std::vector<uint64_t> sums(n, 0);
+  std::deque<int> pending;
+  std::vector<Slot> slots(s->max_inflight);
+  std::vector<int> free_slots;
+  for (int i = s->max_inflight - 1; i >= 0; i--) free_slots.push_back(i);
+  int next = 0, done = 0, rejected = 0, rr = 0;
+  int64_t bytes_done = 0, peak = 0, max_inflight = 0, inflight = 0;
+  const auto t0 = clk::now();
+  auto now_s = [&]() { return std::chrono::duration<double>(clk::now() - t0).count(); };
+  while (done + rejected < n) {
+    bool progress = false;
+    const double t = now_s();
+    while (next < n && reqs[order[next]].arrival_s <= t) pending.push_back(order[next++]);
+    // completions
+    for (int sl = 0; sl < s->max_inflight; sl++) {
+      Slot &S = slots[sl];
+      if (S.req < 0) continue;
+      cudaError_t q = cudaEventQuery(s->events[sl]);
+      if (q == cudaErrorNotReady) continue;
+      if (q != cudaSuccess) return cuda_status(q, "request completion");
+      lat[S.req] = (now_s() - reqs[S.req].arrival_s) * 1e3;
+      sums[S.req] = s->h_sums[sl];
+      bytes_done += S.bytes;
+      s->arena_map.release(S.off, S.bytes);
+      S.req = -1;
+      free_slots.push_back(sl);
+      inflight--;
+      done++;
+      progress = true;
+    }
+    // admissions in arrival order
+    while (!pending.empty() && !free_slots.empty()) {
+      const int ri = pending.front();
+      const t213_request &r = reqs[ri];
+      const int64_t bytes = r.d1 * r.d2 * r.d3 * r.elem_bytes;
+      if (bytes > s->arena_bytes || r.d1 < 0 || r.d2 < 0 || r.d3 < 0) {
+        pending.pop_front();
+        rejected++;
+        progress = true;
+        continue;
+      }
+      if (bytes == 0) {
+        pending.pop_front();
+        lat[ri] = (now_s() - r.arrival_s) * 1e3;
+        done++;
+        progress = true;
+        continue;
+      }
+      const int64_t off = s->arena_map.alloc(bytes);
+      if (off < 0) break;  // wait for memory to free up
+      pending.pop_front();
+      const int sl = free_slots.back();
+      free_slots.pop_back();
+      slots[sl] = Slot{ri, off, bytes};
+      cudaStream_t st = s->streams[rr++ % s->streams.size()];
+      int rc = enqueue_request(s, r, sl, off, st);
+      if (rc) return rc;
+      inflight++;
+      max_inflight = std::max(max_inflight, inflight);
+      peak = std::max(peak, s->arena_map.used());
+      progress = true;
+    }
+    if (!progress) {
+      // nothing to do until the next arrival or completion
+      const double wait = next < n ? reqs[order[next]].arrival_s - now_s() : 0.0;
+      if (wait > 50e-6)
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+      else
+        std::this_thread::yield();
+    }
+  }
+  const double wall = now_s();
+  std::vector<double> ok;
+  for (int i = 0; i < n; i++)
+    if (lat[i] >= 0) ok.push_back(lat[i]);
+  std::sort(ok.begin(), ok.end());
+  auto pct = [&](double p) {
+    if (ok.empty()) return 0.0;
+    size_t k = (size_t)std::min<double>((double)ok.size() - 1, std::ceil(p * ok.size()) - 1);
+    return ok[k];
+  };
+  if (stats) {
+    stats->completed = done;
+    stats->rejected = rejected;
+    stats->bytes_done = bytes_done;
+    stats->p50_ms = pct(0.50);
+    stats->p99_ms = pct(0.99);
+    double sum = 0;
+    for (double v : ok) sum += v;
+    stats->mean_ms = ok.empty() ? 0 : sum / ok.size();
+    stats->max_ms = ok.empty() ? 0 : ok.back();
+    stats->wall_s = wall;
+    stats->peak_resident_bytes = peak;
+    stats->max_inflight = max_inflight;
+  }
+  if (checksums) std::copy(sums.begin(), sums.end(), checksums);
+  if (latency_ms) std::copy(lat.begin(), lat.end(), latency_ms);
+  return T213_OK;
+}
+
+int t213_server_expected_checksum(t213_server s, const t213_request *r, uint64_t *checksum) {
+  if (!s || !r || !checksum) return T213_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = s->streams[0];
+  cudaMemsetAsync(s->d_sums, 0, sizeof(unsigned long long), st);
+  const int64_t nel = r->d1 * r->d2 * r->d3;
+  k_checksum_expected<<<grid_for(nel), 256, 0, st>>>(r->d1, r->d2, r->d3, r->elem_bytes, r->seed, s->d_sums);
+  cudaError_t e = cudaMemcpyAsync(s->h_sums, s->d_sums, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_status(e, "expected checksum");
+  *checksum = s->h_sums[0];
+  return T213_OK;
+}
+
+int t213_server_run_alone(t213_server s, const t213_request *r, uint64_t *checksum) {
+  if (!s || !r || !checksum) return T213_ERR_INVALID_ARGUMENT;
+  const int64_t bytes = r->d1 * r->d2 * r->d3 * r->elem_bytes;
+  if (bytes > s->arena_bytes) {
+    set_error("request larger than the HBM budget");
+    return T213_ERR_BUDGET;
+  }
+  const int64_t off = s->arena_map.alloc(bytes);
+  if (off < 0) return T213_ERR_BUDGET;
+  int rc = enqueue_request(s, *r, 0, off, s->streams[0]);
+  cudaError_t e = cudaStreamSynchronize(s->streams[0]);
+  s->arena_map.release(off, bytes);
+  if (rc) return rc;
+  if (e != cudaSuccess) return cuda_status(e, "run alone");
+  *checksum = s->h_sums[0];
+  return T213_OK;
+}
+
+int t213_server_destroy(t213_server s) {
+  if (!s) return T213_OK;
+  for (cudaStream_t st : s->streams) cudaStreamSynchronize(st);
+  for (cudaEvent_t ev : s->events) cudaEventDestroy(ev);
+  for (cudaStream_t st : s->streams) {
+    release_stream_workspace(st);
+    cudaStreamDestroy(st);
+  }
+  if (s->arena) cudaFree(s->arena);
+  if (s->d_sums) cudaFree(s->d_sums);
+  if (s->h_sums) cudaFreeHost(s->h_sums);
+  delete s;
+  return T213_OK;
+}
+
+}  // extern "C"

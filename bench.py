@@ -234,9 +234,17 @@ def run_ours(args):
         t213.transpose_host(host, D1, D2, D3)
     e2e_s = max_over_ranks(dist, time.perf_counter() - t0)
 
+    del host
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample()
+    batched = serving = None
+    if world == 1 and not args.quick:
+        del x
+        torch.cuda.empty_cache()
+        batched = batched_section(t213, torch, stream)
+        if args.serving:
+            serving = serving_section(t213, torch)
 
     if rank == 0:
         value = world * 2 * nbytes * args.steps / (ms_max * 1e-3) / 1e9
@@ -266,9 +274,80 @@ def run_ours(args):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if batched:
+            line["batched"] = batched
+        if serving:
+            line["serving"] = serving
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+# ------------------------------------------------------ batched / serving ----
+def batched_section(t213, torch, stream):
+    """512 uneven tensors (d1,d2 log-uniform in [16,4096], d3 in {1,2,4,8},
+    fp32/fp64/int32/16-byte, seed 1): one persistent graph-captured launch
+    against the plain call looped over the same list."""
+    w = importlib.import_module("213transpose_b200.workloads")
+    shapes = w.batched_shapes(1, 512)
+    gen = torch.Generator(device="cuda").manual_seed(1)
+    bufs = []
+    for d1, d2, d3, eb, _ in shapes:
+        x = torch.empty(d1 * d2 * d3 * eb, dtype=torch.uint8, device="cuda")
+        x.random_(0, 256, generator=gen)
+        bufs.append(x)
+    B = t213.Batch([(x, d1, d2, d3, eb) for x, (d1, d2, d3, eb, _) in zip(bufs, shapes)])
+
+    def tm(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(reps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            best = min(best, a.elapsed_time(b))
+        return best
+
+    tb, tl = tm(B.execute), tm(B.looped)
+    status = B.status()
+    tot = w.total_bytes(shapes)
+    out = {"workload": "512 tensors, d1,d2 log-uniform [16,4096], d3 in {1,2,4,8}, fp32/fp64/int32/16B, seed 1",
+           "total_GB": round(tot / 1e9, 3), "batched_ms": round(tb, 3), "looped_ms": round(tl, 3),
+           "speedup_vs_looped": round(tl / tb, 3), "batched_GBps": round(2 * tot / tb / 1e6, 1),
+           "looped_GBps": round(2 * tot / tl / 1e6, 1), "device_status": status, "desc": B.describe()}
+    B.close()
+    del bufs
+    torch.cuda.empty_cache()
+    return out
+
+
+def serving_section(t213, torch):
+    """Poisson 2000 req/s, request size log-uniform 1 KB - 2 GB, shapes/dtypes
+    drawn as in the batched workload, 150 GB HBM budget; 2000 requests."""
+    w = importlib.import_module("213transpose_b200.workloads")
+    reqs = w.serving_requests(5, 2000)
+    for i, r in enumerate(reqs):
+        r["seed"] = 1 + i
+    srv = t213.Server(hbm_budget_bytes=150 * 10**9, max_inflight=64, streams=8)
+    srv.run(reqs[:50])  # warm-up: plans of the first shapes
+    stats, sums, lat = srv.run(reqs)
+    bad = sum(1 for r, s in list(zip(reqs, sums))[::40] if s != srv.expected_checksum(r))
+    srv.close()
+    torch.cuda.empty_cache()
+    return {"workload": "Poisson 2000 req/s, log-uniform 1 KB-2 GB, 150 GB budget, 2000 requests",
+            "completed": stats["completed"], "rejected": stats["rejected"],
+            "p50_ms": round(stats["p50_ms"], 3), "p99_ms": round(stats["p99_ms"], 3),
+            "mean_ms": round(stats["mean_ms"], 3), "max_ms": round(stats["max_ms"], 3),
+            "throughput_GBps": round(stats["bytes_done"] / stats["wall_s"] / 1e9, 2),
+            "requests_per_s": round(stats["completed"] / stats["wall_s"], 1),
+            "peak_resident_GB": round(stats["peak_resident_bytes"] / 1e9, 2),
+            "max_inflight": stats["max_inflight"],
+            "latency_includes": "fill of the request tensor on the device (producer stand-in) + in-place transpose",
+            "checksum_mismatches_of_50_sampled": bad}
 
 
 # ----------------------------------------------------------- CPU baseline ----
@@ -353,6 +432,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--quick", action="store_true", help="skip the batched and serving sections")
+    ap.add_argument("--serving", action="store_true", help="also run the 2000-request serving section")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
