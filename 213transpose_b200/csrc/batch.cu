@@ -299,7 +299,9 @@ int t213_batch_create(const t213_tensor_desc *tensors, int32_t count, t213_batch
         }
         case PT_SEG: {
           const CycleTable &ct = *q.table;
-          if ((rc = const_cast<CycleTable &>(ct).ensure_uploaded())) return fail(rc);
+          if ((rc = const_cast<CycleTable &>(ct).ensure_uploaded(nullptr)) ||
+              (rc = const_cast<CycleTable &>(ct).wait_uploaded()))
+            return fail(rc);
           bp.seg_bytes = q.seg_bytes;
           bp.seg_aw = seg_access_width(data, q.seg_bytes, slice_bytes);
           bp.chunks = (const Chunk *)ct.d_chunks;
@@ -409,6 +411,9 @@ int t213_batch_create(const t213_tensor_desc *tensors, int32_t count, t213_batch
   if (e == cudaSuccess) e = cudaMalloc(&B->d_ctrs, (B->n_ctrs + 1) * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMalloc(&B->d_status, 256);
   if (e == cudaSuccess) e = cudaMemset(B->d_status, 0, 256);
+  // the copies and the memset ran on the legacy stream; executes on
+  // non-blocking streams are not ordered after it, so let them land here
+  if (e == cudaSuccess) e = cudaStreamSynchronize(0);
   if (e != cudaSuccess) return fail(cuda_status(e, "batch upload"));
   // workspace the spilled plans need during capture
   for (int i : B->spill) B->spill_ws = std::max(B->spill_ws, plan_workspace_bytes(*B->plans[i]));
@@ -464,7 +469,7 @@ int t213_batch_execute(t213_batch B, t213_stream_t stream) {
     if (B->spill_ws && !workspace(st, B->spill_ws, &rc)) return rc;
     for (int i : B->spill)
       for (const PassDesc &q : B->plans[i]->passes)
-        if (q.table && (rc = q.table->ensure_uploaded())) return rc;
+        if (q.table && ((rc = q.table->ensure_uploaded(st)) || (rc = q.table->wait_uploaded()))) return rc;
     int *w = device_status_word(&rc);
     if (!w) return rc;
   }
@@ -506,7 +511,8 @@ int t213_batch_status(t213_batch B, t213_stream_t stream) {
   e = cudaMemcpy(&v, B->d_status, sizeof(int), cudaMemcpyDeviceToHost);
   if (e != cudaSuccess) return cuda_status(e, "batch status read");
   if (v) {
-    cudaMemset(B->d_status, 0, sizeof(int));
+    if (cudaMemsetAsync(B->d_status, 0, sizeof(int), (cudaStream_t)stream) == cudaSuccess)
+      cudaStreamSynchronize((cudaStream_t)stream);
     set_error("a bounded wait of the persistent batch kernel ran out");
   }
   return v;

@@ -148,8 +148,19 @@ struct CycleTable {
   void *d_carry_items = nullptr;
   int dev = 0;
   std::mutex mu;
-  // Uploads the tables to the device once (synchronous); later calls are free.
-  int ensure_uploaded();
+  // The upload is stream-ordered: a synchronous cudaMemcpy from pageable
+  // memory may return before its DMA lands, and work on non-blocking streams
+  // is not ordered after the legacy stream, so a walker could read a table
+  // that is not there yet.  The first call copies on `st` and records `ready`;
+  // later calls from other streams make their stream wait on `ready` until
+  // the event is seen complete.
+  cudaEvent_t ready = nullptr;
+  cudaStream_t upload_stream = nullptr;
+  bool ready_seen = false;
+  int ensure_uploaded(cudaStream_t st);
+  // Blocks the host until the upload has landed (set-up paths that capture
+  // graphs afterwards call this so captured work needs no event wait).
+  int wait_uploaded();
   ~CycleTable();
 };
 

@@ -467,15 +467,29 @@ __device__ __noinline__ bool bx_seg_walk_tma(const BPass &P, const AnyFn<U> &f, 
     bulk_g2s(buf + (int64_t)b * P.piece_bytes, base + (int64_t)xi * P.seg_bytes, pb, &bars[b]);
     issued++;
   }
-  if (!mbar_wait(&bars[0], parity & 1u)) return false;
+  // on a timeout, wait (bounded) for the loads [waited, issued) still in
+  // flight and drain the stores before giving up
+  int64_t waited = 0;
+  auto give_up = [&]() {
+    for (int64_t j = waited; j < issued; j++) {
+      const int b = (int)(j % NB);
+      if (!mbar_wait(&bars[b], (parity >> b) & 1u)) break;
+      parity ^= 1u << b;
+    }
+    bulk_wait_all<0>();
+    return false;
+  };
+  if (!mbar_wait(&bars[0], parity & 1u)) return give_up();
   parity ^= 1u;
+  waited = 1;
   U last = pos[0];
   for (int64_t s = 1; s <= L; s++) {
     const int bs = (int)(s % NB), bp = (int)((s - 1) % NB);
     U target;
     if (s < L) {
-      if (!mbar_wait(&bars[bs], (parity >> bs) & 1u)) return false;
+      if (!mbar_wait(&bars[bs], (parity >> bs) & 1u)) return give_up();
       parity ^= 1u << bs;
+      waited = s + 1;
       target = pos[bs];
     } else {
       target = f.perm(last);
@@ -649,8 +663,10 @@ __global__ void __launch_bounds__(kBatchThreads, 1)
     if (P.dep_ctr >= 0 && threadIdx.x == 0) {
       volatile unsigned long long *dc = ctrs + P.dep_ctr;
       uint32_t polls = 0;
+      uint64_t t0 = 0;
       while (*dc < (unsigned long long)P.dep_target) {
-        if (++polls > kWaitLimit) {
+        if (polls == 0) t0 = global_ns();
+        if (++polls > kWaitLimit || ((polls & 15) == 0 && global_ns() - t0 > kWaitNs)) {
           s_fail = 1;
           break;
         }

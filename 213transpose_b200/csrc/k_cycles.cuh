@@ -176,12 +176,25 @@ __global__ void __launch_bounds__(32)
       bulk_g2s(buf + (int64_t)b * piece_bytes, base + (int64_t)xi * seg_bytes, pb, &bars[b]);
       issued++;
     }
+    // loads [waited, issued) are in flight; a timed-out walker drains them
+    // (each wait bounded again) before it returns, so no copy still lands in
+    // shared memory of an exited CTA
+    int64_t waited = 0;
+    auto drain = [&]() {
+      for (int64_t j = waited; j < issued; j++) {
+        const int b = (int)(j % NB);
+        if (!mbar_wait(&bars[b], (parity >> b) & 1u)) break;
+        parity ^= 1u << b;
+      }
+    };
     // old value of x_0 in place
     if (!mbar_wait(&bars[0], parity & 1u)) {
       failed = true;
+      drain();
       break;
     }
     parity ^= 1u;
+    waited = 1;
     U last = pos[0];
     for (int64_t s = 1; s <= L; s++) {
       const int bs = (int)(s % NB);
@@ -191,9 +204,11 @@ __global__ void __launch_bounds__(32)
         // x_s must be read before it is overwritten
         if (!mbar_wait(&bars[bs], (parity >> bs) & 1u)) {
           failed = true;
+          drain();
           break;
         }
         parity ^= 1u << bs;
+        waited = s + 1;
         target = pos[bs];
       } else {
         target = dst(last);  // cycle start or the next chunk's start

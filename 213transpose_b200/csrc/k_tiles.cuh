@@ -293,7 +293,15 @@ __global__ void __launch_bounds__(kTileThreads)
     }
   }
   (void)cdiv;
-  if (threadIdx.x == 0 && s_fail) atomicExch(status, 5 /* T213_ERR_TIMEOUT */);
+  if (threadIdx.x == 0 && s_fail) {
+    // loads of iterations [it, it + nbuf) may still be in flight: wait for
+    // them (each wait bounded again) so none lands after the CTA has exited
+    for (int j = it; j < it + nbuf; j++) {
+      if ((int64_t)blockIdx.x + (int64_t)j * gridDim.x >= n_bands) break;
+      if (!mbar_wait(&bars[j % nbuf], (uint32_t)((j / nbuf) & 1))) break;
+    }
+    atomicExch(status, 5 /* T213_ERR_TIMEOUT */);
+  }
 }
 
 }  // namespace t213

@@ -18,14 +18,24 @@ namespace t213 {
 CycleTable::~CycleTable() {
   if (d_chunks) defer_free(dev, d_chunks);
   if (d_carry_items) defer_free(dev, d_carry_items);
+  if (ready) cudaEventDestroy(ready);  // released once the event completes
 }
 
 namespace {
-std::mutex g_grave_mu;
-std::vector<std::pair<int, void *>> g_grave;
+// Never destroyed: tables held by other translation units' caches can be
+// released during static destruction at exit, after this file's statics.
+std::mutex &grave_mu() {
+  static std::mutex *m = new std::mutex;
+  return *m;
+}
+std::vector<std::pair<int, void *>> &grave() {
+  static auto *v = new std::vector<std::pair<int, void *>>;
+  return *v;
+}
 constexpr size_t kGraveMax = 256;
 
 void flush_locked() {
+  auto &g_grave = grave();
   if (g_grave.empty()) return;
   int cur = 0;
   cudaGetDevice(&cur);
@@ -46,13 +56,13 @@ void flush_locked() {
 }  // namespace
 
 void defer_free(int dev, void *p) {
-  std::lock_guard<std::mutex> lk(g_grave_mu);
-  g_grave.push_back({dev, p});
-  if (g_grave.size() > kGraveMax) flush_locked();
+  std::lock_guard<std::mutex> lk(grave_mu());
+  grave().push_back({dev, p});
+  if (grave().size() > kGraveMax) flush_locked();
 }
 
 void flush_deferred_frees() {
-  std::lock_guard<std::mutex> lk(g_grave_mu);
+  std::lock_guard<std::mutex> lk(grave_mu());
   flush_locked();
 }
 
@@ -156,8 +166,9 @@ struct Key {
   int dev;
 };
 
-std::mutex g_mu;
-std::list<std::pair<Key, std::shared_ptr<CycleTable>>> g_cache;  // front = most recent
+// never destroyed, like the plan cache (no CUDA calls from static destructors)
+std::mutex &g_mu = *new std::mutex;
+auto &g_cache = *new std::list<std::pair<Key, std::shared_ptr<CycleTable>>>;  // front = most recent
 constexpr size_t kCacheMax = 256;
 
 }  // namespace
@@ -217,22 +228,55 @@ std::shared_ptr<CycleTable> get_cycle_table(const PermSpec &p, int64_t items_per
   return ct;
 }
 
-int CycleTable::ensure_uploaded() {
+int CycleTable::ensure_uploaded(cudaStream_t st) {
   std::lock_guard<std::mutex> lk(mu);
-  if (n_chunks == 0 || d_chunks) return T213_OK;
-  cudaError_t e = cudaMalloc(&d_chunks, h_chunks.size());
-  if (e == cudaSuccess) e = cudaMemcpy(d_chunks, h_chunks.data(), h_chunks.size(), cudaMemcpyHostToDevice);
+  if (n_chunks == 0) return T213_OK;
+  if (d_chunks) {
+    if (ready_seen) return T213_OK;
+    cudaError_t q = cudaEventQuery(ready);
+    if (q == cudaSuccess) {
+      ready_seen = true;
+      return T213_OK;
+    }
+    if (q != cudaErrorNotReady) return cuda_status(q, "cycle table upload");
+    if (st == upload_stream) return T213_OK;  // same stream: already ordered
+    q = cudaStreamWaitEvent(st, ready, 0);
+    return q == cudaSuccess ? T213_OK : cuda_status(q, "cycle table upload wait");
+  }
+  cudaError_t e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMalloc(&d_chunks, h_chunks.size());
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(d_chunks, h_chunks.data(), h_chunks.size(), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess && n_carry > 0) {
     e = cudaMalloc(&d_carry_items, h_carry_items.size());
     if (e == cudaSuccess)
-      e = cudaMemcpy(d_carry_items, h_carry_items.data(), h_carry_items.size(), cudaMemcpyHostToDevice);
+      e = cudaMemcpyAsync(d_carry_items, h_carry_items.data(), h_carry_items.size(), cudaMemcpyHostToDevice, st);
   }
+  if (e == cudaSuccess) e = cudaEventRecord(ready, st);
   if (e != cudaSuccess) {
+    // nothing reads the tables yet; finish the stream before freeing them
+    cudaStreamSynchronize(st);
     if (d_chunks) cudaFree(d_chunks);
     if (d_carry_items) cudaFree(d_carry_items);
+    if (ready) cudaEventDestroy(ready);
     d_chunks = d_carry_items = nullptr;
+    ready = nullptr;
     return cuda_status(e, "cycle table upload");
   }
+  upload_stream = st;
+  return T213_OK;
+}
+
+int CycleTable::wait_uploaded() {
+  std::lock_guard<std::mutex> lk(mu);
+  if (n_chunks == 0 || ready_seen) return T213_OK;
+  if (!ready) {
+    set_error("cycle table was never uploaded");
+    return T213_ERR_INVALID_ARGUMENT;
+  }
+  cudaError_t e = cudaEventSynchronize(ready);
+  if (e != cudaSuccess) return cuda_status(e, "cycle table upload");
+  ready_seen = true;
   return T213_OK;
 }
 
@@ -250,7 +294,7 @@ int launch_seg_cycles(const CycleTable &ct, char *data, int64_t d3, int64_t slic
                       cudaStream_t st, LaunchStats *ls, char *carry_override, size_t carry_override_bytes) {
   if (ct.n_chunks == 0 || d3 <= 0) return T213_OK;
   {
-    int up = const_cast<CycleTable &>(ct).ensure_uploaded();
+    int up = const_cast<CycleTable &>(ct).ensure_uploaded(st);
     if (up) return up;
   }
   const int aw = seg_access_width(data, seg_bytes, slice_bytes);

@@ -91,6 +91,9 @@ int *device_status_word(int *status) {
   int *p = nullptr;
   cudaError_t e = cudaMalloc(&p, 256);
   if (e == cudaSuccess) e = cudaMemset(p, 0, 256);
+  // the memset runs on the legacy stream, which kernels on non-blocking
+  // streams do not wait for: let it land before any pass can record a status
+  if (e == cudaSuccess) e = cudaStreamSynchronize(0);
   if (e != cudaSuccess) {
     *status = cuda_status(e, "status word");
     return nullptr;
@@ -582,9 +585,12 @@ struct PlanKey {
 // LRU cache of plans (front = most recently used).  Evicting a plan can drop
 // the last reference to its cycle tables; their device memory is then freed
 // only after a device-wide synchronisation (see CycleTable).
-std::mutex g_plan_mu;
-std::list<std::pair<PlanKey, std::shared_ptr<Plan>>> g_plan_lru;
-std::map<PlanKey, std::list<std::pair<PlanKey, std::shared_ptr<Plan>>>::iterator> g_plans;
+// Heap objects that are never destroyed: at process exit the plans (and the
+// CUDA resources of their cycle tables) are left to the driver's teardown
+// instead of being released by static destructors in an unspecified order.
+std::mutex &g_plan_mu = *new std::mutex;
+auto &g_plan_lru = *new std::list<std::pair<PlanKey, std::shared_ptr<Plan>>>;
+auto &g_plans = *new std::map<PlanKey, std::list<std::pair<PlanKey, std::shared_ptr<Plan>>>::iterator>;
 constexpr size_t kPlanCacheMax = 1024;
 
 std::shared_ptr<Plan> new_plan(int64_t d1, int64_t d2, int64_t d3, int eb) {
@@ -1066,7 +1072,9 @@ int t213_device_status(t213_stream_t stream, int32_t *device_status) {
   if (e != cudaSuccess) return cuda_status(e, "cudaStreamSynchronize");
   int v = 0;
   if ((e = cudaMemcpy(&v, w, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) return cuda_status(e, "status read");
-  if (v) cudaMemset(w, 0, sizeof(int));
+  if (v && (e = cudaMemsetAsync(w, 0, sizeof(int), (cudaStream_t)stream)) == cudaSuccess)
+    e = cudaStreamSynchronize((cudaStream_t)stream);
+  if (e != cudaSuccess) return cuda_status(e, "status reset");
   *device_status = v;
   return T213_OK;
 }

@@ -1,14 +1,22 @@
 // Bulk asynchronous copies (TMA, cp.async.bulk) and mbarriers for sm_100a,
-// as inline PTX.  Every wait is bounded: after kWaitLimit polls a wait gives up
-// and the caller records T213_ERR_TIMEOUT in the pass's status word instead of
-// spinning forever.
+// as inline PTX.  Every wait is bounded: after kWaitNs of the global timer (or
+// kWaitLimit polls, whichever comes first) a wait gives up and the caller
+// records T213_ERR_TIMEOUT in the pass's status word instead of spinning
+// forever.
 #pragma once
 
 #include <stdint.h>
 
 namespace t213 {
 
-constexpr uint32_t kWaitLimit = 1u << 24;  // ~1 s of polling with back-off
+constexpr uint32_t kWaitLimit = 1u << 26;          // backstop on the number of polls
+constexpr uint64_t kWaitNs = 2000000000ull;         // 2 s of wall time
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -45,8 +53,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 
 // Bounded wait for the phase with the given parity; false on timeout.
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
   for (uint32_t it = 0; it < kWaitLimit; it++) {
     if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 15) == 15 && global_ns() - t0 > kWaitNs) return false;
     if (it > 32) __nanosleep(64);
   }
   return false;

@@ -53,16 +53,42 @@ def test_admission_under_budget_pressure(t213, cuda):
     srv.close()
 
 
-def test_served_workload_sample(t213, cuda):
-    """The serving configuration's generator (Poisson 2000 req/s, 1 KB-2 GB
-    log-uniform), first 150 requests, 150 GB budget."""
+def test_served_workload(t213, cuda):
+    """The serving configuration: Poisson 2000 req/s, 1 KB-2 GB log-uniform,
+    150 GB budget, 64 in flight on 8 streams, all 2000 requests."""
     w = importlib.import_module("213transpose_b200.workloads")
-    reqs = w.serving_requests(5, 150)
+    reqs = w.serving_requests(5, 2000)
     for i, r in enumerate(reqs):
         r["seed"] = 7 + i
     srv = t213.Server(hbm_budget_bytes=150 * 10**9, max_inflight=64, streams=8)
     stats, sums, lat = srv.run(reqs)
     assert stats["completed"] == len(reqs)
+    assert t213.device_status() == 0
     for r, s in list(zip(reqs, sums))[::5]:
+        assert s == srv.expected_checksum(r), r
+    srv.close()
+
+
+def test_fresh_cycle_tables_on_concurrent_streams(t213, cuda):
+    """Shapes whose plans walk segment cycles, each seen for the first time,
+    all arriving at once on 8 non-blocking streams: a pass must not start
+    before its cycle table has landed on the device."""
+    t213.release_cache()
+    rng = random.Random(11)
+    reqs = []
+    while len(reqs) < 96:
+        eb = rng.choice([4, 8, 16])
+        d3 = rng.choice([1, 2, 4])
+        d1 = int(math.exp(rng.uniform(math.log(16), math.log(20000))))
+        d2 = max(16, int(rng.uniform(2e5, 4e6) / (d1 * d3 * eb)))
+        if "segment_cycles" not in t213.describe(d1, d2, d3, eb):
+            continue
+        reqs.append({"d1": d1, "d2": d2, "d3": d3, "elem_bytes": eb, "t": 0.0, "seed": 500 + len(reqs)})
+    t213.release_cache()
+    srv = t213.Server(hbm_budget_bytes=32 << 30, max_inflight=64, streams=8)
+    stats, sums, lat = srv.run(reqs)
+    assert stats["completed"] == len(reqs)
+    assert t213.device_status() == 0
+    for r, s in zip(reqs, sums):
         assert s == srv.expected_checksum(r), r
     srv.close()
