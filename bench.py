@@ -243,8 +243,7 @@ def run_ours(args):
         del x
         torch.cuda.empty_cache()
         batched = batched_section(t213, torch, stream)
-        if args.serving:
-            serving = serving_section(t213, torch)
+        serving = serving_section(t213, torch)
 
     if rank == 0:
         value = world * 2 * nbytes * args.steps / (ms_max * 1e-3) / 1e9
@@ -433,7 +432,6 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--quick", action="store_true", help="skip the batched and serving sections")
-    ap.add_argument("--serving", action="store_true", help="also run the 2000-request serving section")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
