@@ -70,6 +70,7 @@ _SIGS = {
     "t213_skinny_r2c_transpose": ([_vp, _i64, _i64, _i64, _i32, _vp], ctypes.c_int),
     "t213_rotate": ([_i32, _pi64, _i32, _vp, _i64, _i64, _i64, _i32, _vp], ctypes.c_int),
     "t213_row_shuffle": ([_i32, _pi64, _i32, _vp, _i64, _i64, _i64, _i32, _vp], ctypes.c_int),
+    "t213_row_shuffle_noalloc": ([_i32, _pi64, _i32, _vp, _i64, _i64, _i64, _i32, _vp], ctypes.c_int),
     "t213_col_shuffle": ([_i32, _pi64, _i32, _vp, _i64, _i64, _i64, _i32, _vp], ctypes.c_int),
     "t213_scatter_permute": ([_i32, _pi64, _i32, _vp, _i64, _i64, _i64, _i32, _vp], ctypes.c_int),
     "t213_transpose_host": ([_vp, _i64, _i64, _i64, _i32, _vp], ctypes.c_int),

@@ -32,7 +32,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-
                      "--expt-relaxed-constexpr"]
 
 LIB_SOURCES = ["runtime.cu", "launch_gather.cu", "launch_cycles.cu", "launch_tiles.cu", "host_io.cu",
-               "tuner.cu", "batch.cu", "serve.cu"]
+               "tuner.cu", "batch.cu", "serve.cu", "noalloc.cu"]
 CXX_API_SOURCES = ["cxx_api.cu"]
 
 
