@@ -10,6 +10,8 @@
 //                shared memory (a band is at most one CTA's shared memory).
 #pragma once
 
+#include <cuda.h>
+
 #include "common.cuh"
 #include "tma.cuh"
 
@@ -183,6 +185,205 @@ __global__ void __launch_bounds__(kTileThreads)
       if (!cdiag) __stcs(reinterpret_cast<uint4 *>(cs + (car + w) * n + cac) + ch, ob.v);
     }
     __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Tile swap fed by TMA.  Persistent CTAs of NCW consumer warps plus one
+// producer warp (the last).  The producer's lane 0 loads tile pairs with tiled
+// TMA copies (3-D boxes of TS rows x 128 bytes, 128-byte swizzle) into a ring
+// of NS stages, up to NS pairs ahead of the consumers.  All consumer warps
+// work on the same stage: each thread takes Q x Q blocks (Q = 16 / EB
+// elements, one 16-byte chunk wide) of the pair, reads the block's Q rows,
+// swaps it in registers and stores Q 16-byte vectors into the partner tile's
+// place.  The eight lanes of each quarter-warp read eight different chunks of
+// one row, which the swizzle puts in eight different bank groups, and each
+// store instruction of a warp writes 64 contiguous bytes in each of eight
+// output rows.  Every consumer waits on every stage in order and each warp
+// releases it once (the empty barrier counts NCW arrivals), so each parity
+// wait is at most one phase ahead.
+//
+// The data map views every slice as an m x (n * EB) byte matrix (dims
+// {n*EB, m, d3}).  A pair is read completely before either of its tiles is
+// written and no two CTAs share a pair, so the pass is in place.  Every wait
+// is bounded; on timeout the CTA records T213_ERR_TIMEOUT, waits for its own
+// loads in flight and returns.
+// ---------------------------------------------------------------------------
+// Pair p of a block's nt x nt tile grid (p < nt*(nt+1)/2) -> tiles (x, y),
+// x <= y, ordered by super-tiles of grp x grp tiles (grp divides nt): first
+// the grp*grp pairs of each off-diagonal super-tile pair (X < Y, row-major
+// over the super-grid's strict upper triangle), then the grp*(grp+1)/2 pairs
+// inside each diagonal super-tile.  Consecutive pairs -- the ones concurrent
+// CTAs take -- then cover a grp-tile-wide region on both sides of the
+// diagonal, so the rows read and written on either side are grp tiles long.
+__device__ __forceinline__ void tile_pair_decode(uint32_t p, uint32_t nt, uint32_t grp, uint32_t &x, uint32_t &y) {
+  const uint32_t nsup = nt / grp, gsq = grp * grp;
+  const uint32_t off = nsup * (nsup - 1) / 2 * gsq;
+  if (p < off) {
+    const uint32_t sp = p / gsq, r = p - sp * gsq;
+    uint32_t X, Yp;
+    tri_decode32(sp, nsup - 1, X, Yp);
+    const uint32_t xi = r / grp, yi = r - xi * grp;
+    x = X * grp + xi;
+    y = (Yp + 1) * grp + yi;
+  } else {
+    const uint32_t p2 = p - off, gd = grp * (grp + 1) / 2;
+    const uint32_t D = p2 / gd, r = p2 - D * gd;
+    uint32_t xi, yi;
+    tri_decode32(r, grp, xi, yi);
+    x = D * grp + xi;
+    y = D * grp + yi;
+  }
+}
+
+template <int EB, int TS_>
+struct TileTma {
+  static constexpr int TS = TS_;                    // tile side in elements
+  static constexpr int NBOX = TS * EB / 128;        // 128-byte boxes per tile row
+  static constexpr int BOX_BYTES = TS * 128;        // one box: TS rows of 128 bytes
+  static constexpr int TILE_BYTES = TS * TS * EB;
+  static constexpr int Q = 16 / EB;                 // elements per 16-byte chunk
+  static constexpr int NQ = TS / Q;                 // Q x Q blocks per tile side
+  static constexpr int BLOCKS = NQ * NQ;
+  static_assert(NBOX >= 1 && TS * EB % 128 == 0, "a tile row is whole 128-byte boxes");
+  static_assert(NQ % 8 == 0 && BLOCKS % 32 == 0, "block mapping needs 8 | NQ");
+};
+
+template <int EB, int TS>
+__global__ void __launch_bounds__(1024)
+    k_tile_swap_tma(const __grid_constant__ CUtensorMap tmap, char *__restrict__ data, int64_t n,
+                    int64_t slice_elems, uint32_t total, int64_t t, FastDiv<uint32_t> fd_per_slice,
+                    FastDiv<uint32_t> fd_pairs, FastDiv<uint32_t> fd_Bn, uint32_t nt, uint32_t grp, int ns,
+                    int *status) {
+  using E = typename ElemT<EB>::type;
+  using TT = TileTma<EB, TS>;
+  constexpr int Q = TT::Q, NQ = TT::NQ;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  // barriers first, then the 1024-byte aligned stages (swizzle atoms)
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem_raw);
+  uint64_t *empty = full + ns;
+  const uint32_t base_u = smem_u32(smem_raw);
+  unsigned char *stages = smem_raw + (((base_u + 16 * ns + 1023) & ~1023u) - base_u);
+  __shared__ int s_fail, s_issued;
+  const int ncw = (int)(blockDim.x >> 5) - 1;  // consumer warps
+  const int nct = ncw * 32;                     // consumer threads
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    s_fail = 0;
+    s_issued = 0;
+    for (int i = 0; i < ns; i++) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], (uint32_t)ncw);
+    }
+    fence_barrier_init();
+  }
+  __syncthreads();
+
+  // pair u -> slice k, block (I, J), tiles (x, y) and (y, x)
+  auto decode = [&](uint32_t u, uint32_t &k, uint32_t &I, uint32_t &J, uint32_t &x, uint32_t &y) {
+    k = fd_per_slice.div(u);
+    const uint32_t r = u - k * fd_per_slice.get();
+    const uint32_t blk = fd_pairs.div(r);
+    const uint32_t p = r - blk * fd_pairs.get();
+    I = fd_Bn.div(blk);
+    J = blk - I * fd_Bn.get();
+    tile_pair_decode(p, nt, grp, x, y);
+  };
+
+  if (warp == ncw) {
+    // ---------------------------------------------------------- producer --
+    if (lane == 0) {
+      prefetch_tmap(&tmap);
+      int li = 0;  // pairs issued so far
+      for (uint32_t u = blockIdx.x; u < total; u += gridDim.x, li++) {
+        const int s = li % ns;
+        if (li >= ns && !mbar_wait(&empty[s], (uint32_t)(((li / ns) - 1) & 1))) {
+          s_fail = 1;
+          break;
+        }
+        if (*(volatile int *)&s_fail) break;
+        uint32_t k, I, J, x, y;
+        decode(u, k, I, J, x, y);
+        const bool diag = (x == y);
+        unsigned char *sA = stages + (size_t)s * 2 * TT::TILE_BYTES;
+        mbar_expect_tx(&full[s], diag ? TT::TILE_BYTES : 2 * TT::TILE_BYTES);
+        const int32_t rowA = (int32_t)(I * (uint32_t)t + x * TS), colA = (int32_t)(J * (uint32_t)t + y * TS);
+        const int32_t rowB = (int32_t)(I * (uint32_t)t + y * TS), colB = (int32_t)(J * (uint32_t)t + x * TS);
+#pragma unroll
+        for (int b = 0; b < TT::NBOX; b++)
+          tma_load_3d(sA + b * TT::BOX_BYTES, &tmap, colA * EB + b * 128, rowA, (int32_t)k, &full[s]);
+        if (!diag) {
+#pragma unroll
+          for (int b = 0; b < TT::NBOX; b++)
+            tma_load_3d(sA + TT::TILE_BYTES + b * TT::BOX_BYTES, &tmap, colB * EB + b * 128, rowB, (int32_t)k,
+                        &full[s]);
+        }
+      }
+      s_issued = li;
+    }
+  } else {
+    // --------------------------------------------------------- consumers --
+    E *d = reinterpret_cast<E *>(data);
+    int li = 0;
+    for (uint32_t u = blockIdx.x; u < total; u += gridDim.x, li++) {
+      const int s = li % ns;
+      // every lane waits (each gets the barrier's acquire); the warp leaves
+      // together if any lane's bounded wait ran out
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&full[s], (uint32_t)((li / ns) & 1)));
+      if (!ok) {
+        if (lane == 0) s_fail = 1;
+        break;
+      }
+      uint32_t k, I, J, x, y;
+      decode(u, k, I, J, x, y);
+      const bool diag = (x == y);
+      E *blk0 = d + (int64_t)k * slice_elems + ((int64_t)I * t) * n + (int64_t)J * t;
+      const unsigned char *sA = stages + (size_t)s * 2 * TT::TILE_BYTES;
+      const int nblk = (diag ? 1 : 2) * TT::BLOCKS;
+      // block g of the pair: tile h = g / BLOCKS (0: A at (x, y), 1: B at
+      // (y, x)); source tile (sx, sy) is written transposed to tile (sy, sx)
+#pragma unroll 2
+      for (int g = threadIdx.x; g < nblk; g += nct) {
+        const int h = g >= TT::BLOCKS;
+        const int q = g - h * TT::BLOCKS;
+        const unsigned char *src = sA + h * TT::TILE_BYTES;
+        const uint32_t sx = h ? y : x, sy = h ? x : y;
+        E *dst = blk0 + (int64_t)(sy * TS) * n + sx * TS;  // rows sy*TS.., cols sx*TS..
+        const int cbl = q & 7, rbl = (q >> 3) & 3, rest = q >> 5;
+        const int cb = (rest % (NQ / 8)) * 8 + cbl;
+        const int rb = (rest / (NQ / 8)) * 4 + rbl;
+        union V {
+          uint4 v;
+          E e[Q];
+        } in[Q], out[Q];
+#pragma unroll
+        for (int i = 0; i < Q; i++) {
+          const int r = rb * Q + i;
+          const int bx = cb >> 3, cc = cb & 7;
+          in[i].v = *reinterpret_cast<const uint4 *>(src + bx * TT::BOX_BYTES + r * 128 + ((cc ^ (r & 7)) << 4));
+        }
+#pragma unroll
+        for (int i = 0; i < Q; i++)
+#pragma unroll
+          for (int j = 0; j < Q; j++) out[j].e[i] = in[i].e[j];
+#pragma unroll
+        for (int j = 0; j < Q; j++)
+          __stcs(reinterpret_cast<uint4 *>(dst + (int64_t)(cb * Q + j) * n) + rb, out[j].v);
+      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&empty[s]);
+    }
+  }
+  __syncthreads();
+  if (s_fail && threadIdx.x == nct) {
+    // wait for every load this CTA issued (each wait bounded again) so none
+    // lands in shared memory after the CTA has exited
+    const int issued = s_issued;
+    for (int s = 0; s < ns && s < issued; s++) {
+      const int last = s + ((issued - 1 - s) / ns) * ns;  // last use of stage s that was issued
+      if (!mbar_wait(&full[s], (uint32_t)((last / ns) & 1))) break;
+    }
+    atomicExch(status, 5 /* T213_ERR_TIMEOUT */);
   }
 }
 

@@ -94,6 +94,28 @@ __device__ __forceinline__ void bulk_wait_all() {
   asm volatile("cp.async.bulk.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// Plain arrive on an mbarrier (consumer release of a pipeline stage).
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Tiled TMA load of one box of a 3-D tensor map into shared memory
+// (cp.async.bulk.tensor, no multicast), completion counted on bar.  The x
+// coordinate is in elements of the map's data type and must be a multiple of
+// 16 bytes.
+__device__ __forceinline__ void tma_load_3d(void *dst_smem, const void *tmap, int32_t x, int32_t y, int32_t z,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(dst_smem)),
+      "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void prefetch_tmap(const void *tmap) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(tmap) : "memory");
+}
+
 // Ampere-style asynchronous 4/8/16-byte copies global -> shared (LDGSTS):
 // many in flight per thread without holding registers.
 template <int N>
