@@ -2,11 +2,15 @@
 // arena, continuous dispatch of admitted requests onto a stream pool,
 // completion polling and latency statistics.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -203,6 +207,72 @@ int enqueue_request(t213_server s, const t213_request &r, int slot, int64_t off,
   return e == cudaSuccess ? T213_OK : cuda_status(e, "request launch");
 }
 
+// Plans requests on worker threads as they arrive, so that the dispatch loop
+// only looks plans up: building a new shape's plan (its cycle tables above
+// all) takes from microseconds to tens of milliseconds of host time, which a
+// single dispatch thread would otherwise spend while the GPU idles.
+class PlannerPool {
+ public:
+  PlannerPool(int dev, int threads, const t213_request *reqs, int n) : reqs_(reqs), planned_(n) {
+    for (auto &f : planned_) f.store(0, std::memory_order_relaxed);
+    for (int i = 0; i < threads; i++)
+      workers_.emplace_back([this, dev] {
+        cudaSetDevice(dev);
+        for (;;) {
+          int ri;
+          {
+            std::unique_lock<std::mutex> lk(mu_);
+            cv_.wait(lk, [&] { return stop_ || !queue_.empty(); });
+            if (queue_.empty()) return;
+            ri = queue_.front();
+            queue_.pop_front();
+          }
+          const t213_request &r = reqs_[ri];
+          int st = T213_OK;
+          if (r.d1 > 0 && r.d2 > 0 && r.d3 > 0 &&
+              (r.elem_bytes == 1 || r.elem_bytes == 2 || r.elem_bytes == 4 || r.elem_bytes == 8 || r.elem_bytes == 16))
+            get_plan(r.d1, r.d2, r.d3, r.elem_bytes, r.plan_kind, 0, &st);  // errors resurface at dispatch
+          planned_[ri].store(1, std::memory_order_release);
+        }
+      });
+  }
+  ~PlannerPool() {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      stop_ = true;
+      queue_.clear();
+    }
+    cv_.notify_all();
+    for (auto &w : workers_) w.join();
+  }
+  void submit(int ri) {
+    {
+      std::lock_guard<std::mutex> lk(mu_);
+      queue_.push_back(ri);
+    }
+    cv_.notify_one();
+  }
+  bool ready(int ri) const { return planned_[ri].load(std::memory_order_acquire) != 0; }
+
+ private:
+  const t213_request *reqs_;
+  std::vector<std::atomic<int>> planned_;
+  std::vector<std::thread> workers_;
+  std::mutex mu_;
+  std::condition_variable cv_;
+  std::deque<int> queue_;
+  bool stop_ = false;
+};
+
+// Planner threads: T213_SERVE_PLANNERS, else all host threads but two (at
+// most 16, at least 1).
+int planner_threads() {
+  const char *v = std::getenv("T213_SERVE_PLANNERS");
+  if (v && std::atoi(v) > 0) return std::min(64, std::atoi(v));
+  const int hw = (int)std::thread::hardware_concurrency();
+  return std::max(1, std::min(16, hw - 2));
+}
+
 }  // namespace
 
 extern "C" {
@@ -272,12 +342,16 @@ int t213_server_run(t213_server s, const t213_request *reqs, int32_t n, t213_ser
   for (int i = s->max_inflight - 1; i >= 0; i--) free_slots.push_back(i);
   int next = 0, done = 0, rejected = 0, rr = 0;
   int64_t bytes_done = 0, peak = 0, max_inflight = 0, inflight = 0;
+  PlannerPool planners(s->dev, planner_threads(), reqs, n);
   const auto t0 = clk::now();
   auto now_s = [&]() { return std::chrono::duration<double>(clk::now() - t0).count(); };
   while (done + rejected < n) {
     bool progress = false;
     const double t = now_s();
-    while (next < n && reqs[order[next]].arrival_s <= t) pending.push_back(order[next++]);
+    while (next < n && reqs[order[next]].arrival_s <= t) {
+      planners.submit(order[next]);
+      pending.push_back(order[next++]);
+    }
     // completions
     for (int sl = 0; sl < s->max_inflight; sl++) {
       Slot &S = slots[sl];
@@ -295,27 +369,35 @@ int t213_server_run(t213_server s, const t213_request *reqs, int32_t n, t213_ser
       done++;
       progress = true;
     }
-    // admissions in arrival order
-    while (!pending.empty() && !free_slots.empty()) {
-      const int ri = pending.front();
+    // admissions in arrival order among the requests whose plans are ready
+    // (a request still being planned is passed over, not waited for; the
+    // first one that does not fit the arena stops admission until memory
+    // frees up, so large requests are not starved)
+    size_t pi = 0;
+    while (pi < pending.size() && pi < 256 && !free_slots.empty()) {
+      const int ri = pending[pi];
       const t213_request &r = reqs[ri];
       const int64_t bytes = r.d1 * r.d2 * r.d3 * r.elem_bytes;
       if (bytes > s->arena_bytes || r.d1 < 0 || r.d2 < 0 || r.d3 < 0) {
-        pending.pop_front();
+        pending.erase(pending.begin() + pi);
         rejected++;
         progress = true;
         continue;
       }
       if (bytes == 0) {
-        pending.pop_front();
+        pending.erase(pending.begin() + pi);
         lat[ri] = (now_s() - r.arrival_s) * 1e3;
         done++;
         progress = true;
         continue;
       }
+      if (!planners.ready(ri)) {
+        pi++;
+        continue;
+      }
       const int64_t off = s->arena_map.alloc(bytes);
       if (off < 0) break;  // wait for memory to free up
-      pending.pop_front();
+      pending.erase(pending.begin() + pi);
       const int sl = free_slots.back();
       free_slots.pop_back();
       slots[sl] = Slot{ri, off, bytes};

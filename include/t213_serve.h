@@ -4,9 +4,11 @@
  *
  * A server replays an open-loop request schedule against the GPU: each request
  * names a (d1,d2,d3) tensor of elem_bytes elements and an arrival time.  On
- * arrival a request waits in FIFO order until its tensor fits the HBM budget
- * (the tensor itself, in place: no scratch copy of the full tensor) and an
- * in-flight slot is free; it is then admitted into a device arena reserved at
+ * arrival a request is planned on a host worker thread (T213_SERVE_PLANNERS,
+ * default all host threads but two, at most 16), then waits, in arrival order
+ * among the planned requests, until its tensor fits the HBM budget (the tensor
+ * itself, in place: no scratch copy of the full tensor) and an in-flight slot
+ * is free; it is then admitted into a device arena reserved at
  * creation, its tensor is materialised on the device (a seeded fill standing in
  * for the producer), transposed in place on one of the server's streams, and
  * checksummed.  Admitted requests run concurrently on the stream pool while new
