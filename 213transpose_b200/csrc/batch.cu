@@ -42,7 +42,10 @@ struct t213_batch_st {
 
 namespace {
 
-constexpr int64_t kItemBytes = 1024 * 1024;  // target bytes read per queue item
+// Target bytes read per queue item: small enough that one tensor's pass
+// spreads over many SMs (the batch's critical path is the chain of passes of
+// its slowest tensor), large enough that the queue overhead stays small.
+constexpr int64_t kItemBytes = 256 * 1024;
 
 // Tensors above this size saturate the GPU on their own and keep their
 // specialised kernels (graph nodes); smaller ones share the persistent kernel.
@@ -382,12 +385,11 @@ int t213_batch_create(const t213_tensor_desc *tensors, int32_t count, t213_batch
         case BK_CARRY:
           upi = per(bp.seg_bytes);
           break;
-        case BK_SEG: {
-          const int64_t avg_len = std::max<int64_t>(1, (bp.n_chunks ? (B->plans[i]->passes.empty() ? 1 : 1) : 1));
-          (void)avg_len;
-          upi = std::max<int64_t>(kBatchWarps, per(bp.piece_bytes * 8) / kBatchWarps * kBatchWarps);
+        case BK_SEG:
+          // one chunk walk per warp: a walk is a chain of dependent loads,
+          // so walks are spread over CTAs rather than queued behind each other
+          upi = kBatchWarps;
           break;
-        }
       }
       for (int64_t u = 0; u < bp.n_units; u += upi) {
         B->h_items.push_back(BItem{pi, 0, u, std::min(bp.n_units, u + upi)});

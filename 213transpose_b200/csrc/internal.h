@@ -111,6 +111,9 @@ int launch_row_gather(const FnSpec &f, char *data, int64_t d3, int64_t m, int64_
                       cudaStream_t st, LaunchStats *ls);
 // Describes the variant launch_col_gather / launch_row_gather would pick.
 std::string describe_col_gather(int64_t m, int64_t n, int eb, const void *data);
+// The variant launch_col_gather picks for this functor (the cluster-local
+// kernel when the functor's form and the strip halo allow it).
+std::string describe_col_gather_fn(const FnSpec &f, int64_t m, int64_t n, int eb, const void *data);
 std::string describe_row_gather(int64_t m, int64_t n, int eb, const void *data);
 // Number of launches the gathers enqueue.
 int count_col_gather(int64_t d3, int64_t m, int64_t n, int eb);

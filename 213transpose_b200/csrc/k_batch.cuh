@@ -41,8 +41,8 @@ __device__ __forceinline__ void cp_async_wait_group() {
 
 constexpr int kBatchThreads = 512;
 constexpr int kBatchWarps = kBatchThreads / 32;
-constexpr int kBatchRing = 3;                 // TMA buffers per walker warp
-constexpr int64_t kBatchPiece = 4096;         // bytes per TMA walker piece
+constexpr int kBatchRing = 6;                 // TMA buffers per walker warp
+constexpr int64_t kBatchPiece = 2048;         // bytes per TMA walker piece
 constexpr int64_t kBatchSmem = 192 * 1024;    // dynamic shared memory per CTA
 constexpr int64_t kBatchBarBytes = 1024;      // mbarriers live at the front
 
@@ -419,20 +419,48 @@ __device__ __noinline__ void bx_row(const BPass &P, const AnyFn<U> &f, int64_t u
 }
 
 // ----------------------------------------------------------------- CARRY ----
-__device__ __noinline__ void bx_carry(const BPass &P, int64_t u0, int64_t u1) {
-  // unit = one (carry item, slice): copy seg_bytes in 16-byte (or 1-byte) words
-  const int aw = P.seg_aw;
-  for (int64_t u = u0; u < u1; u++) {
+// unit = one (carry item, slice) segment.  The words of all the item's units
+// are spread over every thread of the CTA (segments can be a few words long),
+// with four loads in flight per thread before their stores.
+template <int AW>
+__device__ __forceinline__ void bx_carry_words(const BPass &P, int64_t u0, int64_t u1) {
+  using W = typename WordT<AW>::type;
+  const int64_t wps = P.seg_bytes / AW;
+  const int64_t total = (u1 - u0) * wps;
+  auto addr = [&](int64_t w, const W *&src, W *&dst) {
+    const int64_t u = u0 + w / wps, word = w % wps;
     const int64_t ii = u / P.d3, k = u - ii * P.d3;
     const CarryItem ci = P.carries[ii];
-    const char *src = P.data + k * P.slice_bytes + ci.pos * P.seg_bytes;
-    char *dst = P.carry_buf + (ci.slot * P.d3 + k) * P.seg_bytes;
-    if (aw == 16) {
-      for (int64_t w = threadIdx.x; w < P.seg_bytes / 16; w += blockDim.x)
-        reinterpret_cast<uint4 *>(dst)[w] = __ldcg(reinterpret_cast<const uint4 *>(src) + w);
-    } else {
-      for (int64_t w = threadIdx.x; w < P.seg_bytes; w += blockDim.x) dst[w] = src[w];
+    src = reinterpret_cast<const W *>(P.data + k * P.slice_bytes + ci.pos * P.seg_bytes) + word;
+    dst = reinterpret_cast<W *>(P.carry_buf + (ci.slot * P.d3 + k) * P.seg_bytes) + word;
+  };
+  constexpr int UNR = 4;
+  const int64_t step = (int64_t)blockDim.x * UNR;
+  for (int64_t w0 = threadIdx.x; w0 < total; w0 += step) {
+    const W *src[UNR];
+    W *dst[UNR];
+    W v[UNR];
+#pragma unroll
+    for (int q = 0; q < UNR; q++) {
+      const int64_t w = w0 + (int64_t)q * blockDim.x;
+      if (w < total) {
+        addr(w, src[q], dst[q]);
+        v[q] = __ldcg(src[q]);
+      }
     }
+#pragma unroll
+    for (int q = 0; q < UNR; q++)
+      if (w0 + (int64_t)q * blockDim.x < total) *dst[q] = v[q];
+  }
+}
+
+__device__ __noinline__ void bx_carry(const BPass &P, int64_t u0, int64_t u1) {
+  switch (P.seg_aw) {
+    case 16: bx_carry_words<16>(P, u0, u1); break;
+    case 8: bx_carry_words<8>(P, u0, u1); break;
+    case 4: bx_carry_words<4>(P, u0, u1); break;
+    case 2: bx_carry_words<2>(P, u0, u1); break;
+    default: bx_carry_words<1>(P, u0, u1); break;
   }
 }
 
@@ -527,7 +555,7 @@ __device__ __noinline__ void bx_seg_walk_reg(const BPass &P, const AnyFn<U> &f, 
   U pos = (U)ch.start;
   W cur = (ch.carry >= 0) ? *reinterpret_cast<const W *>(P.carry_buf + (ch.carry * P.d3 + k) * P.seg_bytes + off)
                           : __ldcg(reinterpret_cast<const W *>(base + (int64_t)pos * P.seg_bytes));
-  constexpr int UNR = 4;
+  constexpr int UNR = 8;
   int64_t remaining = ch.len;
   while (remaining > 0) {
     const int cnt = remaining < UNR ? (int)remaining : UNR;

@@ -117,6 +117,76 @@ __global__ void __launch_bounds__(kGatherThreads)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Row gather with the next unit's load in flight: a unit (one or more whole
+// rows, at most half the CTA's shared memory) is copied into one of two
+// buffers with cp.async groups while the previous unit is gathered from the
+// other buffer and written back, so each CTA keeps its loads and its stores
+// going at the same time.  Units are this CTA's, in order; a buffer is
+// refilled only after the barrier that ends the gather reading it.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async_commit_grp() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_grp1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+template <int EB, int AW, typename F, typename U>
+__global__ void __launch_bounds__(kGatherThreads)
+    k_row_pipe(char *__restrict__ data, int64_t total_rows, U m, U n, int rows_per_unit, int64_t buf_bytes,
+               FastDiv<U> words_per_row, FastDiv<U> mdiv, F fn) {
+  using E = typename ElemT<EB>::type;
+  using W = typename WordT<AW>::type;
+  using P = Pack<AW, EB>;
+  constexpr int PER = AW / EB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int64_t n_units = (total_rows + rows_per_unit - 1) / rows_per_unit;
+  const int64_t row_bytes = (int64_t)n * EB;
+
+  auto stage = [&](int64_t u, unsigned char *buf) {
+    const int64_t r0 = u * rows_per_unit;
+    const int nr = (int)min((int64_t)rows_per_unit, total_rows - r0);
+    const W *g = reinterpret_cast<const W *>(data + r0 * row_bytes);
+    W *sw = reinterpret_cast<W *>(buf);
+    const uint32_t nw = (uint32_t)((int64_t)nr * (n / PER));
+#pragma unroll 4
+    for (uint32_t w = threadIdx.x; w < nw; w += blockDim.x) {
+      if constexpr (AW >= 4)
+        cp_async<AW>(sw + w, g + w);
+      else
+        sw[w] = __ldcs(g + w);
+    }
+    cp_async_commit_grp();
+  };
+
+  int64_t u = blockIdx.x;
+  if (u >= n_units) return;
+  stage(u, smem_raw);
+  for (int it = 0; u < n_units; u += gridDim.x, it++) {
+    unsigned char *cur = smem_raw + (it & 1) * buf_bytes;
+    const int64_t un = u + gridDim.x;
+    if (un < n_units)
+      stage(un, smem_raw + ((it + 1) & 1) * buf_bytes);
+    else
+      cp_async_commit_grp();  // an empty group keeps the wait count uniform
+    cp_async_wait_grp1();     // this thread's copies of the current unit have landed
+    __syncthreads();          // and every other thread's
+    const int64_t r0 = u * rows_per_unit;
+    const int nr = (int)min((int64_t)rows_per_unit, total_rows - r0);
+    W *g = reinterpret_cast<W *>(data + r0 * row_bytes);
+    const E *sm = reinterpret_cast<const E *>(cur);
+    const uint32_t nw = (uint32_t)((int64_t)nr * (n / PER));
+    const U i_base = (U)(r0 % (int64_t)m);
+    for (uint32_t w = threadIdx.x; w < nw; w += blockDim.x) {
+      const U rr = words_per_row.div((U)w);
+      const U j0 = ((U)w - rr * words_per_row.get()) * PER;
+      const U i = mdiv.mod(i_base + rr);
+      typename P::U pk;
+#pragma unroll
+      for (int e = 0; e < PER; e++) pk.e[e] = sm[(int64_t)rr * n + fn(i, j0 + e)];
+      __stcs(g + w, pk.w);
+    }
+    __syncthreads();  // the buffer is restaged two units later
+  }
+}
+
 // Rows too long for a cluster: the old rows were copied to `scratch` by the
 // host (one device-to-device copy per group of rows); this kernel gathers from
 // that copy in global memory (L2-resident for groups up to tens of MB).
@@ -230,6 +300,218 @@ __global__ void __launch_bounds__(kGatherThreads)
       cg::this_cluster().sync();
     else
       __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Cluster-local column gather.  Every column functor of the decomposition has
+// one of two forms:
+//   src(i, j) = (pi(i) + r(j)) mod m       rotators, fused pre/post-ops of C2R
+//                                           and the R2C fused post-op
+//   src(i, j) = p((i - j) mod m)           the R2C fused pre-op
+// Written in a key space kappa (kappa = pi(i), or kappa = i), the source row of
+// output (kappa, column j0 + w) of a strip is F((kappa + r_w) mod m), with F
+// the identity or p and r_w = r(j0 + w) (or -(j0 + w)) varying by at most a
+// few rows across the W columns of the strip.  So the keys [k0, k1) of one CTA
+// need only the source rows F(k0 + r_0 + dmin ... k1 + r_0 + dmax): the CTA's
+// share of the strip plus a halo of (dmax - dmin) rows.  The CTAs of a cluster
+// split the keys, each loads its rows (halo included) into its own shared
+// memory, the cluster barrier orders every load of the strip before any
+// store, and each CTA writes its output rows G(kappa) (G = pi^-1 or the
+// identity) from its own shared memory.  No element crosses DSMEM; the
+// strips can be 128-256 bytes wide however tall the matrix is.  A strip short
+// enough for one CTA is held whole instead: slot = key, no halo, and the
+// source slot of (kappa, w) is (kappa + r_w) mod m.
+//
+// The loops keep the index work per element small: a lane owns one word
+// (16 bytes, or one element) of every row it touches, evaluates F or G once
+// for 32 rows and passes the results around by shuffles, and reads the
+// per-column shifts once per strip.
+// ---------------------------------------------------------------------------
+template <typename U>
+struct MapId {
+  T213_HD U operator()(U x) const { return x; }
+};
+
+// Key offset of column j: the column functor at row 0 (form 1 with pi(0) = 0).
+template <typename U, typename F>
+struct OffOfCol {
+  F f;
+  T213_HD U operator()(U j) const { return f((U)0, j); }
+};
+
+// Key offset +-(j mod m) (C2R fused post-op: +j; R2C fused pre-op: -j).
+template <typename U, bool NEG>
+struct OffAffine {
+  FastDiv<U> m;
+  T213_HD U operator()(U j) const {
+    const U r = m.mod(j);
+    return NEG ? (r ? m.get() - r : 0) : r;
+  }
+};
+
+constexpr int kColHaloMax = 64;  // largest halo (dmax - dmin) a strip may need
+
+template <int EB, int AW, typename U, typename Off, typename Fsrc, typename Gout, bool CLUSTER>
+__global__ void __launch_bounds__(kGatherThreads)
+    k_col_local(char *__restrict__ data, int64_t d3, U m, U n, U W, U WS, int64_t n_strips, U H, int halo, Off off,
+                Fsrc F, Gout G, int *status) {
+  using E = typename ElemT<EB>::type;
+  using Wd = typename WordT<AW>::type;
+  using P = Pack<AW, EB>;
+  constexpr int PER = AW / EB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  E *sm = reinterpret_cast<E *>(smem_raw);
+  __shared__ int s_sh[256];  // per column of the strip: slot shift (halo mode) or key offset r_w (whole mode)
+  __shared__ int s_span;
+  __shared__ U s_base;
+
+  int rank = 0, K = 1;
+  int64_t unit0 = blockIdx.x, ustride = gridDim.x;
+  if (CLUSTER) {
+    cg::cluster_group cl = cg::this_cluster();
+    rank = (int)cl.block_rank();
+    K = (int)cl.num_blocks();
+    unit0 = blockIdx.x / K;
+    ustride = gridDim.x / K;
+  }
+  // whole mode: one CTA owns every key of the strip, slot = key, no halo
+  const bool whole = !CLUSTER && H >= m;
+  const int64_t n_units = d3 * n_strips;
+  const U k0 = (U)min((int64_t)rank * (int64_t)H, (int64_t)m);
+  const U k1 = (U)min((int64_t)k0 + (int64_t)H, (int64_t)m);
+  const U nk = k1 - k0;
+  const int64_t pitch = (int64_t)n * EB;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+
+  for (int64_t u = unit0; u < n_units; u += ustride) {
+    const int64_t k = u / n_strips;
+    const U s = (U)(u - k * n_strips);
+    const U j0 = s * W;
+    const U wn = min(W, n - j0);  // multiple of PER
+    const uint32_t wpr = (uint32_t)(wn / PER);
+    char *sbase = data + (k * (int64_t)m * n + j0) * EB;
+    // ---- per-strip column offsets -------------------------------------------
+    if (warp == 0) {
+      const int64_t mm = (int64_t)m;
+      const int64_t r0 = (int64_t)off(j0);
+      int dmin = 0, dmax = 0;
+      for (U w = lane; w < wn; w += 32) {
+        const int64_t rw = (int64_t)off(j0 + w);
+        int64_t d = rw - r0;
+        if (2 * d > mm) d -= mm;
+        if (2 * d <= -mm) d += mm;
+        s_sh[w] = whole ? (int)rw : (int)d;
+        dmin = min(dmin, (int)d);
+        dmax = max(dmax, (int)d);
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        dmin = min(dmin, __shfl_xor_sync(0xffffffffu, dmin, o));
+        dmax = max(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+      }
+      __syncwarp();
+      if (!whole)
+        for (U w = lane; w < wn; w += 32) s_sh[w] -= dmin;
+      if (lane == 0) {
+        s_span = whole ? 0 : dmax - dmin;
+        int64_t b = whole ? 0 : ((int64_t)k0 + r0 + dmin) % mm;
+        if (b < 0) b += mm;
+        s_base = (U)b;
+      }
+    }
+    __syncthreads();
+    // the host sized shared memory for its own scan of every strip's span;
+    // a strip that needs more records an error and moves no data
+    const bool fits = s_span <= halo;
+    if (!fits && threadIdx.x == 0) atomicExch(status, 1 /* T213_ERR_INVALID_ARGUMENT */);
+    const U nslots = !fits ? 0 : whole ? m : (nk > 0 ? nk + (U)s_span : 0);
+    const U nout = fits ? nk : 0;
+    const U base = s_base;
+    auto key_of_slot = [&](U sl) -> U {
+      U key = base + sl;
+      return key >= m ? key - m : key;
+    };
+    auto slot_of = [&](U o, int sh) -> U {  // source slot of output o for a column with shift sh
+      if (whole) {
+        U v = k0 + o + (U)sh;  // key + r_w < 2m
+        return v >= m ? v - m : v;
+      }
+      return o + (U)sh;
+    };
+    if (32 % wpr == 0) {
+      // ---- fast path: a lane keeps one word of the strip's rows; the row maps
+      // are evaluated once per lane for 32 rows and broadcast by shuffles
+      const uint32_t rpi = 32 / wpr, lr = lane / wpr, lw = lane - lr * wpr;
+      int sh[PER];
+#pragma unroll
+      for (int e = 0; e < PER; e++) sh[e] = s_sh[lw * PER + e];
+      for (U sb = (U)warp * 32; sb < nslots; sb += (U)nwarps * 32) {
+        const U mys = sb + lane;
+        const U myrow = mys < nslots ? F(key_of_slot(mys)) : 0;
+        for (uint32_t r = lr; r < 32; r += rpi) {
+          const U row = __shfl_sync(0xffffffffu, myrow, r);
+          const U sl = sb + r;
+          if (sl < nslots) {
+            const Wd *gp = reinterpret_cast<const Wd *>(sbase + (int64_t)row * pitch) + lw;
+            Wd *dp = reinterpret_cast<Wd *>(sm + (int64_t)sl * WS) + lw;
+            if constexpr (AW >= 4)
+              cp_async<AW>(dp, gp);
+            else
+              *dp = __ldcs(gp);
+          }
+        }
+      }
+      if constexpr (AW >= 4) cp_async_wait_all();
+      // every CTA of the strip has read its rows before anyone writes
+      if (CLUSTER)
+        cg::this_cluster().sync();
+      else
+        __syncthreads();
+      for (U ob = (U)warp * 32; ob < nout; ob += (U)nwarps * 32) {
+        const U myo = ob + lane;
+        const U myrow = myo < nout ? G(k0 + myo) : 0;
+        for (uint32_t r = lr; r < 32; r += rpi) {
+          const U row = __shfl_sync(0xffffffffu, myrow, r);
+          const U o = ob + r;
+          if (o < nout) {
+            typename P::U pk;
+#pragma unroll
+            for (int e = 0; e < PER; e++) pk.e[e] = sm[(int64_t)slot_of(o, sh[e]) * WS + lw * PER + e];
+            __stcs(reinterpret_cast<Wd *>(sbase + (int64_t)row * pitch) + lw, pk.w);
+          }
+        }
+      }
+    } else {
+      // ---- any strip width (the last, narrower strip) -------------------------
+      const uint32_t nw = (uint32_t)nslots * wpr;
+      for (uint32_t t = threadIdx.x; t < nw; t += blockDim.x) {
+        const uint32_t sl = t / wpr, w = t - sl * wpr;
+        const U row = F(key_of_slot((U)sl));
+        const Wd *gp = reinterpret_cast<const Wd *>(sbase + (int64_t)row * pitch) + w;
+        if constexpr (AW >= 4)
+          cp_async<AW>(reinterpret_cast<Wd *>(sm + (int64_t)sl * WS) + w, gp);
+        else
+          reinterpret_cast<Wd *>(sm + (int64_t)sl * WS)[w] = __ldcs(gp);
+      }
+      if constexpr (AW >= 4) cp_async_wait_all();
+      if (CLUSTER)
+        cg::this_cluster().sync();
+      else
+        __syncthreads();
+      const uint32_t nwo = (uint32_t)nout * wpr;
+      for (uint32_t t = threadIdx.x; t < nwo; t += blockDim.x) {
+        const uint32_t o = t / wpr, w = t - o * wpr;
+        const U row = G(k0 + (U)o);
+        typename P::U pk;
+#pragma unroll
+        for (int e = 0; e < PER; e++) {
+          const int c = (int)(w * PER + e);
+          pk.e[e] = sm[(int64_t)slot_of((U)o, s_sh[c]) * WS + c];
+        }
+        __stcs(reinterpret_cast<Wd *>(sbase + (int64_t)row * pitch) + w, pk.w);
+      }
+    }
+    __syncthreads();  // shared memory and s_sh are reused by the next strip
   }
 }
 

@@ -3,9 +3,14 @@
 // index width, and the functor dispatch.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 
-#include "internal.h"
 #include "k_gather.cuh"
+#include "plan.h"
 
 namespace t213 {
 
@@ -73,10 +78,31 @@ struct ColCfg {
   int64_t group_w = 0;    // scratch fallback: columns per copy
 };
 
+int env_int(const char *name) {
+  const char *v = std::getenv(name);
+  return v ? std::atoi(v) : 0;
+}
+
 ColCfg col_config(int64_t m, int64_t n, int eb, const void *data) {
   ColCfg c;
   c.aw = pick_aw(eb, data, n * eb, 0);
   const int64_t P = c.aw / eb;
+  // T213_COL_WBYTES / T213_COL_CLUSTER force a strip width (bytes) and a
+  // cluster size, for measuring the variants against each other
+  if (const int fw = env_int("T213_COL_WBYTES")) {
+    const int fk = std::max(1, std::min(kMaxCluster, env_int("T213_COL_CLUSTER")));
+    const int64_t W = round_up(std::min<int64_t>(std::max<int64_t>(P, fw / eb), round_up(n, P)), P);
+    const int64_t WS = (W * eb) % 128 == 0 ? W + P : W;
+    const int64_t H = (m + fk - 1) / fk;
+    if (H * WS * eb <= kSmemCap) {
+      c.W = W;
+      c.WS = WS;
+      c.K = fk;
+      c.H = fk == 1 ? m : H;
+      c.smem = c.H * WS * eb;
+      return c;
+    }
+  }
   auto strip = [&](int64_t wbytes, bool widen) -> int64_t {
     int64_t W = std::max<int64_t>(P, wbytes / eb);
     if (widen) {  // short columns: widen so a unit is worth ~48 KB
@@ -125,6 +151,162 @@ ColCfg col_config(int64_t m, int64_t n, int eb, const void *data) {
   return c;
 }
 
+// ------------------------------------------------- cluster-local columns --
+// Which form a column functor has (k_col_local): 1 = offset of the functor
+// itself, identity maps; 2 = C2R fused post-op (+j offsets, output rows through
+// the inverse post-permuter); 3 = R2C fused pre-op (-j offsets, source rows
+// through the pre-permuter); 0 = not handled.
+int local_form(int kind) {
+  switch (kind) {
+    case T213_FN_C2R_PREROTATOR:
+    case T213_FN_C2R_POSTROTATOR:
+    case T213_FN_R2C_PREROTATOR:
+    case T213_FN_R2C_POSTROTATOR:
+    case T213_FN_C2R_FUSED_PREOP:
+    case T213_FN_R2C_FUSED_POSTOP:
+      return 1;
+    case T213_FN_C2R_FUSED_POSTOP:
+      return 2;
+    case T213_FN_R2C_FUSED_PREOP:
+      return 3;
+  }
+  return 0;
+}
+
+struct LocalCfg {
+  bool ok = false;
+  int aw = 4, K = 1;
+  int64_t W = 0, WS = 0, H = 0, halo = 0, smem = 0;
+  bool u64 = false;
+};
+
+// Largest (dmax - dmin) over the strips of width W: the key offsets of one
+// strip, unwrapped around the strip's first column, as the kernel computes
+// them.  O(n) functor evaluations, cached per (functor, m, n, W).
+template <typename Off>
+int64_t strip_span(Off off, int64_t m, int64_t n, int64_t W) {
+  int64_t worst = 0;
+  for (int64_t j0 = 0; j0 < n; j0 += W) {
+    const int64_t r0 = (int64_t)off((uint64_t)j0);
+    int64_t lo = 0, hi = 0;
+    for (int64_t w = 1; w < W && j0 + w < n; w++) {
+      int64_t d = (int64_t)off((uint64_t)(j0 + w)) - r0;
+      if (2 * d > m) d -= m;
+      if (2 * d <= -m) d += m;
+      lo = std::min(lo, d);
+      hi = std::max(hi, d);
+    }
+    worst = std::max(worst, hi - lo);
+    if (worst > kColHaloMax) break;
+  }
+  return worst;
+}
+
+int64_t local_span(const FnSpec &f, int64_t m, int64_t n, int64_t W) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t, int64_t>, int64_t> cache;
+  const auto key = std::make_tuple(f.kind, f.p[0], f.p[1], f.p[2], f.p[3], m, n, W);
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+  }
+  int64_t span = kColHaloMax + 1;
+  const int form = local_form(f.kind);
+  if (form == 2) {
+    span = strip_span(OffAffine<uint64_t, false>{FastDiv<uint64_t>((uint64_t)m)}, m, n, W);
+  } else if (form == 3) {
+    span = strip_span(OffAffine<uint64_t, true>{FastDiv<uint64_t>((uint64_t)m)}, m, n, W);
+  } else if (form == 1) {
+    with_col_fn<uint64_t>(f, m, [&](auto fn) -> bool {
+      using F = decltype(fn);
+      span = strip_span(OffOfCol<uint64_t, F>{fn}, m, n, W);
+      return true;
+    });
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if (cache.size() > 4096) cache.clear();
+  cache[key] = span;
+  return span;
+}
+
+int64_t gcd64(int64_t a, int64_t b) {
+  while (b) {
+    const int64_t t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+
+// The forms hold for the decomposition's own parameters: the functor's m is
+// the matrix's, c = gcd(m, n') (the post-permuter is then a bijection whose
+// inverse is the pre-permuter with q = b^-1 mod a), and the pre-permuter's q
+// is a unit mod a.  Other parameters keep plain gather semantics through the
+// staged kernel.
+bool local_params_ok(const FnSpec &f, int64_t m) {
+  switch (f.kind) {
+    case T213_FN_C2R_FUSED_PREOP:
+    case T213_FN_R2C_FUSED_POSTOP:
+      return f.p[0] == m && f.p[1] > 0;
+    case T213_FN_C2R_FUSED_POSTOP:
+      return f.p[0] == m && f.p[1] > 0 && f.p[2] > 0 && f.p[2] == gcd64(m, f.p[1]);
+    case T213_FN_R2C_FUSED_PREOP:
+      return f.p[2] == m && f.p[0] > 0 && f.p[1] > 0 && f.p[0] * f.p[1] == m && f.p[3] >= 0 &&
+             gcd64(f.p[3] % f.p[0], f.p[0]) == 1;
+  }
+  return true;  // rotators: any amount is a rotation of the m-row column
+}
+
+LocalCfg local_col_config(const FnSpec &f, int64_t m, int64_t n, int eb, const void *data) {
+  LocalCfg c;
+  const char *var = std::getenv("T213_COL_VARIANT");
+  if (var && std::strcmp(var, "old") == 0) return c;
+  if (!local_form(f.kind) || m <= 0 || n <= 0 || !local_params_ok(f, m)) return c;
+  c.aw = pick_aw(eb, data, n * eb, 0);
+  const int64_t P = c.aw / eb;
+  // strip width: a power of two of access words, at most 32 of them (the
+  // kernel's fast path gives each lane one word of a row) and 256 elements
+  auto width = [&](int64_t wbytes) {
+    int64_t words = 1;
+    while (words < 32 && 2 * words * c.aw <= wbytes && 2 * words * P <= 256) words *= 2;
+    return std::min<int64_t>(words * P, round_up(n, P));
+  };
+  // index width: the functor's own bound, and the permutation maps' products
+  // (below a * a with a = m / gcd)
+  c.u64 = !fits32(f, m, n) || (double)m * (double)m >= 2.0e9;
+  const int64_t whole_cap = (env_int("T213_COL_WHOLE_KB") > 0 ? env_int("T213_COL_WHOLE_KB") : 104) * 1024;
+  if (m * 128 <= whole_cap && env_int("T213_COL_LOCAL_K") <= 1) {
+    // whole strips in one CTA: at least 128-byte rows, widened to about
+    // 48 KB per strip (at most 256 columns), no halo
+    c.W = width(std::max<int64_t>(128, (48 * 1024) / m));
+    while (c.W > P && m * c.W * eb > whole_cap) c.W /= 2;
+    c.WS = c.W;
+    c.K = 1;
+    c.H = m;
+    c.halo = 0;
+    c.smem = m * c.WS * eb;
+    c.ok = true;
+    return c;
+  }
+  const int64_t wbytes = env_int("T213_COL_LOCAL_WBYTES") > 0 ? env_int("T213_COL_LOCAL_WBYTES") : 128;
+  c.W = width(wbytes);
+  c.WS = c.W;  // the gather's diagonal reads step by WS +- 1 words: no padding needed
+  c.halo = local_span(f, m, n, c.W);
+  if (c.halo > kColHaloMax) return c;
+  const int64_t target = (env_int("T213_COL_LOCAL_SMEM_KB") > 0 ? env_int("T213_COL_LOCAL_SMEM_KB") : 100) * 1024;
+  const int64_t row_bytes = c.WS * eb;
+  const int64_t hmax = std::max<int64_t>(1, target / row_bytes - c.halo);
+  c.K = (int)std::min<int64_t>(kMaxCluster + 1, (m + hmax - 1) / hmax);
+  if (env_int("T213_COL_LOCAL_K") > 1) c.K = env_int("T213_COL_LOCAL_K");
+  if (c.K > kMaxCluster || c.K < 2) return c;
+  c.H = (m + c.K - 1) / c.K;
+  c.smem = (c.H + c.halo) * row_bytes;
+  if (c.smem > kSmemCap) return c;
+  c.ok = true;
+  return c;
+}
+
 // --------------------------------------------------------------- row config --
 struct RowCfg {
   int aw = 4;
@@ -133,6 +315,8 @@ struct RowCfg {
   int64_t part = 0;   // elements per CTA when clustered
   int64_t smem = 0;
   int64_t group_rows = 0;
+  bool pipe = false;  // k_row_pipe: two buffers of buf_bytes
+  int64_t buf_bytes = 0;
 };
 
 RowCfg row_config(int64_t m, int64_t n, int eb, const void *data) {
@@ -140,6 +324,23 @@ RowCfg row_config(int64_t m, int64_t n, int eb, const void *data) {
   r.aw = pick_aw(eb, data, n * eb, 0);
   const int64_t P = r.aw / eb;
   const int64_t row_bytes = n * eb;
+  // Double-buffered units of whole rows (k_row_pipe, T213_ROW_STAGE_KB per
+  // buffer), on request with T213_ROW_VARIANT=pipe.  Measured on B200 it is
+  // not the default: the staged kernel's two or three resident CTAs per SM
+  // already overlap one CTA's loads with another's gather (fp64 (7919, 6151,
+  // 2) C2R shuffle 0.345 ms staged against 0.388 ms double-buffered; R2C
+  // shuffle 0.291 against 0.284 ms; fp32 (8192, 6143, 2) 0.212 against 0.209).
+  const char *var = std::getenv("T213_ROW_VARIANT");
+  const int64_t stage = (env_int("T213_ROW_STAGE_KB") > 0 ? env_int("T213_ROW_STAGE_KB") : 48) * 1024;
+  const int64_t cap = std::max<int64_t>(stage, (kSmemCap / 2) / 16 * 16);
+  if (var && std::strcmp(var, "pipe") == 0 && row_bytes <= cap) {
+    r.K = 1;
+    r.pipe = true;
+    r.rows_per_unit = (int)std::max<int64_t>(1, std::min<int64_t>(m, stage / row_bytes));
+    r.buf_bytes = round_up(r.rows_per_unit * row_bytes, 16);
+    r.smem = 2 * r.buf_bytes;
+    return r;
+  }
   if (row_bytes <= kSmemCap) {
     r.K = 1;
     int64_t rpu = std::max<int64_t>(1, (48 * 1024) / row_bytes);
@@ -237,6 +438,17 @@ bool fits32(const FnSpec &f, int64_t m, int64_t n) {
 }
 
 // ------------------------------------------------------------------ column --
+std::string describe_col_gather_fn(const FnSpec &f, int64_t m, int64_t n, int eb, const void *data) {
+  LocalCfg lc = local_col_config(f, m, n, eb, data);
+  if (lc.ok) {
+    char buf[160];
+    snprintf(buf, sizeof buf, "col_local[W=%lld cluster=%d halo=%lld smem=%lldK aw=%d]", (long long)lc.W, lc.K,
+             (long long)lc.halo, (long long)(lc.smem / 1024), lc.aw);
+    return buf;
+  }
+  return describe_col_gather(m, n, eb, data);
+}
+
 std::string describe_col_gather(int64_t m, int64_t n, int eb, const void *data) {
   ColCfg c = col_config(m, n, eb, data);
   char buf[160];
@@ -256,9 +468,77 @@ int count_col_gather(int64_t d3, int64_t m, int64_t n, int eb) {
   return (int)(2 * groups * d3);
 }
 
+namespace {
+
+// k_col_local for one element size / access width / index width.
+template <int EB, int AW, typename U>
+int launch_col_local_t(const FnSpec &f, const LocalCfg &c, char *data, int64_t d3, int64_t m, int64_t n,
+                       cudaStream_t st) {
+  const int64_t n_strips = (n + c.W - 1) / c.W;
+  const int64_t units = n_strips * d3;
+  int status = T213_OK;
+  auto go = [&](auto off, auto F, auto G) {
+    using Off = decltype(off);
+    using Fs = decltype(F);
+    using Gs = decltype(G);
+    int *stw = device_status_word(&status);
+    if (!stw) return;
+    if (c.K == 1) {
+      auto kern = k_col_local<EB, AW, U, Off, Fs, Gs, false>;
+      if ((status = prep_kernel(kern, c.smem, 1))) return;
+      const int64_t grid = persistent_grid(kern, kGatherThreads, c.smem, 1, units);
+      status = launch_k(kern, grid, kGatherThreads, c.smem, 1, st, data, d3, (U)m, (U)n, (U)c.W, (U)c.WS, n_strips,
+                        (U)c.H, (int)c.halo, off, F, G, stw);
+    } else {
+      auto kern = k_col_local<EB, AW, U, Off, Fs, Gs, true>;
+      if ((status = prep_kernel(kern, c.smem, c.K))) return;
+      const int64_t grid = persistent_grid(kern, kGatherThreads, c.smem, c.K, units);
+      status = launch_k(kern, grid, kGatherThreads, c.smem, c.K, st, data, d3, (U)m, (U)n, (U)c.W, (U)c.WS,
+                        n_strips, (U)c.H, (int)c.halo, off, F, G, stw);
+    }
+  };
+  const int form = local_form(f.kind);
+  if (form == 1) {
+    with_col_fn<U>(f, m, [&](auto fn) -> bool {
+      go(OffOfCol<U, decltype(fn)>{fn}, MapId<U>{}, MapId<U>{});
+      return true;
+    });
+  } else if (form == 2) {  // p = {m, n', c}
+    const int64_t cc = f.p[2] > 0 ? f.p[2] : 1, a = m / cc, b = f.p[1] / cc;
+    int64_t binv = 0;
+    if (a > 1) {
+      ext_gcd(b % a, a, &binv);
+      binv %= a;
+      if (binv < 0) binv += a;
+    }
+    go(OffAffine<U, false>{FastDiv<U>((uint64_t)m)}, MapId<U>{}, PermR2CPre<U>(m, cc, binv));
+  } else {  // form 3, p = {a, c, m, q}
+    const int64_t cc = f.p[1] > 0 ? f.p[1] : 1, a = f.p[0] > 0 ? f.p[0] : 1;
+    const int64_t q = ((f.p[3] % a) + a) % a;
+    go(OffAffine<U, true>{FastDiv<U>((uint64_t)m)}, PermR2CPre<U>(m, cc, q), MapId<U>{});
+  }
+  return status;
+}
+
+}  // namespace
+
 int launch_col_gather(const FnSpec &f, char *data, int64_t d3, int64_t m, int64_t n, int eb,
                       cudaStream_t st, LaunchStats *ls) {
   if (m <= 0 || n <= 0 || d3 <= 0) return T213_OK;
+  const LocalCfg lc = local_col_config(f, m, n, eb, data);
+  if (lc.ok) {
+    int status = T213_ERR_UNSUPPORTED;
+    auto run = [&](auto EBc, auto AWc) -> bool {
+      constexpr int EB = decltype(EBc)::value;
+      constexpr int AW = decltype(AWc)::value;
+      status = lc.u64 ? launch_col_local_t<EB, AW, uint64_t>(f, lc, data, d3, m, n, st)
+                      : launch_col_local_t<EB, AW, uint32_t>(f, lc, data, d3, m, n, st);
+      return true;
+    };
+    dispatch_eb_aw(eb, lc.aw, run);
+    if (ls) ls->launches++;
+    return status;
+  }
   ColCfg c = col_config(m, n, eb, data);
   const bool u32 = fits32(f, m, n);
   int status = T213_OK;
@@ -335,6 +615,9 @@ std::string describe_row_gather(int64_t m, int64_t n, int eb, const void *data) 
   char buf[160];
   if (r.K == 0)
     snprintf(buf, sizeof buf, "row_gather[scratch rows/group=%lld aw=%d]", (long long)r.group_rows, r.aw);
+  else if (r.pipe)
+    snprintf(buf, sizeof buf, "row_gather[pipelined rows/unit=%d smem=2x%lldK aw=%d]", r.rows_per_unit,
+             (long long)(r.buf_bytes / 1024), r.aw);
   else if (r.K == 1)
     snprintf(buf, sizeof buf, "row_gather[rows/unit=%d smem=%lldK aw=%d]", r.rows_per_unit,
              (long long)(r.smem / 1024), r.aw);
@@ -369,6 +652,16 @@ int launch_row_gather(const FnSpec &f, char *data, int64_t d3, int64_t m, int64_
         known = true;
         FastDiv<U> wpr((uint64_t)(n / PER));
         FastDiv<U> md((uint64_t)m);
+        if (r.pipe) {
+          auto kern = k_row_pipe<EB, AW, F, U>;
+          if ((status = prep_kernel(kern, r.smem, 1))) return true;
+          const int64_t units = (total_rows + r.rows_per_unit - 1) / r.rows_per_unit;
+          int64_t grid = persistent_grid(kern, kGatherThreads, r.smem, 1, units);
+          status = launch_k(kern, grid, kGatherThreads, r.smem, 1, st, data, total_rows, (U)m, (U)n,
+                            r.rows_per_unit, r.buf_bytes, wpr, md, fn);
+          if (ls) ls->launches++;
+          return true;
+        }
         if (r.K == 1) {
           auto kern = k_row_gather<EB, AW, F, U, false>;
           if ((status = prep_kernel(kern, r.smem, 1))) return true;

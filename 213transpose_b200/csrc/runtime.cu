@@ -321,7 +321,11 @@ std::string fmt_plan(const Plan &P) {
     s += " ";
     switch (p.type) {
       case PT_COL:
-        snprintf(buf, sizeof buf, "col_gather(fn=%d)%s", p.fn.kind, describe_col_gather(p.m, p.n, P.eb, nullptr).substr(10).c_str());
+        {
+          const std::string d = describe_col_gather_fn(p.fn, p.m, p.n, P.eb, nullptr);
+          snprintf(buf, sizeof buf, "%s(fn=%d)%s", d.substr(0, d.find('[')).c_str(), p.fn.kind,
+                   d.substr(d.find('[')).c_str());
+        }
         break;
       case PT_ROW:
         snprintf(buf, sizeof buf, "row_gather(fn=%d)%s", p.fn.kind, describe_row_gather(p.m, p.n, P.eb, nullptr).substr(10).c_str());
@@ -384,7 +388,8 @@ void r2c_passes(Plan &P, int64_t m, int64_t n, bool skinny) {
 
 double gather_cost(const PassDesc &p, int eb) {
   if (p.type == PT_COL) {
-    std::string d = describe_col_gather(p.m, p.n, eb, nullptr);
+    std::string d = describe_col_gather_fn(p.fn, p.m, p.n, eb, nullptr);
+    if (d.find("col_local") == 0) return 1 / 0.6;
     if (d.find("scratch") != std::string::npos) return 1 / 0.2;
     if (d.find("cluster=1 ") != std::string::npos) return 1 / 0.45;
     return 1 / 0.3;
