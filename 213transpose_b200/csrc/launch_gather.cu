@@ -442,7 +442,7 @@ std::string describe_col_gather_fn(const FnSpec &f, int64_t m, int64_t n, int eb
   LocalCfg lc = local_col_config(f, m, n, eb, data);
   if (lc.ok) {
     char buf[160];
-    snprintf(buf, sizeof buf, "col_local[W=%lld cluster=%d halo=%lld smem=%lldK aw=%d]", (long long)lc.W, lc.K,
+    snprintf(buf, sizeof buf, "col_gather[local W=%lld cluster=%d halo=%lld smem=%lldK aw=%d]", (long long)lc.W, lc.K,
              (long long)lc.halo, (long long)(lc.smem / 1024), lc.aw);
     return buf;
   }

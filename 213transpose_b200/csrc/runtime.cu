@@ -389,7 +389,7 @@ void r2c_passes(Plan &P, int64_t m, int64_t n, bool skinny) {
 double gather_cost(const PassDesc &p, int eb) {
   if (p.type == PT_COL) {
     std::string d = describe_col_gather_fn(p.fn, p.m, p.n, eb, nullptr);
-    if (d.find("col_local") == 0) return 1 / 0.6;
+    if (d.find("[local") != std::string::npos) return 1 / 0.6;
     if (d.find("scratch") != std::string::npos) return 1 / 0.2;
     if (d.find("cluster=1 ") != std::string::npos) return 1 / 0.45;
     return 1 / 0.3;
