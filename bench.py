@@ -208,6 +208,22 @@ def run_ours(args):
     achieved = 2 * nbytes / (dom_ms * 1e-3) / 1e9
     traffic = ncu_traffic(dom)
 
+    # out-of-place comparison point: torch's transpose(-2, -1) copied into a
+    # second buffer (one read and one write of every byte, twice the memory)
+    oop = torch.empty_like(x)
+    xv, ov = x.view(D3, D2, D1), oop.view(D3, D1, D2)
+    for _ in range(args.warmup):
+        ov.copy_(xv.transpose(1, 2))
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(args.steps):
+        ov.copy_(xv.transpose(1, 2))
+    b.record(stream)
+    b.synchronize()
+    ms_oop = a.elapsed_time(b) / args.steps
+    del oop, xv, ov
+    torch.cuda.empty_cache()
+
     # secondary tensor: fp64 (7919, 6151, 2)
     nb2 = D1B * D2B * D3B * EBB
     y = torch.empty(D1B * D2B * D3B, dtype=torch.float64, device=dev).uniform_(-1, 1, generator=gen)
@@ -265,6 +281,10 @@ def run_ours(args):
             "secondary": {"workload": f"fp64 (7919,6151,2) {nb2 / 1e6:.1f} MB",
                           "plan": t213.describe(D1B, D2B, D3B, EBB),
                           "value": round(world * 2 * nb2 * args.steps / (ms_b * 1e-3) / 1e9, 1), "unit": UNIT},
+            "out_of_place_torch": {"what": "torch x.view(d3,d2,d1).transpose(1,2) copied into a second buffer "
+                                           "(out of place: one sweep, 2x memory)",
+                                   "ms": round(ms_oop, 4), "GBps": round(2 * nbytes / (ms_oop * 1e-3) / 1e9, 1),
+                                   "in_place_vs_out_of_place_time": round((ms_max / args.steps) / ms_oop, 3)},
             "e2e": {"value": round(world * 2 * nbytes * e2e_steps / e2e_s / 1e9, 2), "unit": UNIT,
                     "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                     "path": "t213_transpose_host (pinned host memory, slices pipelined over copy engines)"},
