@@ -8,6 +8,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <vector>
 
 #include "k_gather.cuh"
 #include "plan.h"
@@ -289,21 +290,34 @@ LocalCfg local_col_config(const FnSpec &f, int64_t m, int64_t n, int eb, const v
     c.ok = true;
     return c;
   }
-  const int64_t wbytes = env_int("T213_COL_LOCAL_WBYTES") > 0 ? env_int("T213_COL_LOCAL_WBYTES") : 128;
-  c.W = width(wbytes);
-  c.WS = c.W;  // the gather's diagonal reads step by WS +- 1 words: no padding needed
-  c.halo = local_span(f, m, n, c.W);
-  if (c.halo > kColHaloMax) return c;
-  const int64_t target = (env_int("T213_COL_LOCAL_SMEM_KB") > 0 ? env_int("T213_COL_LOCAL_SMEM_KB") : 100) * 1024;
-  const int64_t row_bytes = c.WS * eb;
-  const int64_t hmax = std::max<int64_t>(1, target / row_bytes - c.halo);
-  c.K = (int)std::min<int64_t>(kMaxCluster + 1, (m + hmax - 1) / hmax);
-  if (env_int("T213_COL_LOCAL_K") > 1) c.K = env_int("T213_COL_LOCAL_K");
-  if (c.K > kMaxCluster || c.K < 2) return c;
-  c.H = (m + c.K - 1) / c.K;
-  c.smem = (c.H + c.halo) * row_bytes;
-  if (c.smem > kSmemCap) return c;
-  c.ok = true;
+  // tall strips: 128-byte strips over a cluster of up to 16 CTAs of about
+  // 100 KB each; taller columns take narrower strips and fuller CTAs (still
+  // far ahead of the DSMEM-gathering and global-scratch variants)
+  struct Try {
+    int64_t wbytes, kb;
+  };
+  std::vector<Try> tries;
+  if (env_int("T213_COL_LOCAL_WBYTES") > 0 || env_int("T213_COL_LOCAL_SMEM_KB") > 0)
+    tries.push_back({env_int("T213_COL_LOCAL_WBYTES") > 0 ? env_int("T213_COL_LOCAL_WBYTES") : 128,
+                     env_int("T213_COL_LOCAL_SMEM_KB") > 0 ? env_int("T213_COL_LOCAL_SMEM_KB") : 100});
+  else
+    tries = {{128, 100}, {128, 200}, {64, 200}, {32, 200}, {16, 200}};
+  for (const Try &t : tries) {
+    c.W = width(t.wbytes);
+    c.WS = c.W;  // the gather's diagonal reads step by WS +- 1 words: no padding needed
+    c.halo = local_span(f, m, n, c.W);
+    if (c.halo > kColHaloMax) continue;
+    const int64_t row_bytes = c.WS * eb;
+    const int64_t hmax = std::max<int64_t>(1, (t.kb * 1024) / row_bytes - c.halo);
+    c.K = (int)std::min<int64_t>(kMaxCluster + 1, (m + hmax - 1) / hmax);
+    if (env_int("T213_COL_LOCAL_K") > 1) c.K = env_int("T213_COL_LOCAL_K");
+    if (c.K > kMaxCluster || c.K < 2) continue;
+    c.H = (m + c.K - 1) / c.K;
+    c.smem = (c.H + c.halo) * row_bytes;
+    if (c.smem > kSmemCap) continue;
+    c.ok = true;
+    return c;
+  }
   return c;
 }
 
@@ -349,16 +363,23 @@ RowCfg row_config(int64_t m, int64_t n, int eb, const void *data) {
     r.smem = r.rows_per_unit * row_bytes;
     return r;
   }
+  // Rows longer than shared memory: copied to the stream's workspace in
+  // groups of about T213_ROW_GROUP_MB (default 64) and gathered from there,
+  // mostly out of L2.  Measured on B200 this beats splitting each row over a
+  // thread-block cluster and gathering element by element through DSMEM
+  // (T213_ROW_VARIANT=cluster): 3.4-3.6 ms against 10.1 ms for the R2C row
+  // pass of (89, 675165, 8) fp32, 3.7 against 7.9 ms on (344, 359054, 4).
   int K = (int)((row_bytes + kSmemTarget - 1) / kSmemTarget);
   if (K > kMaxCluster) K = (int)((row_bytes + kSmemCap - 1) / kSmemCap);
-  if (K <= kMaxCluster) {
+  if (K <= kMaxCluster && var && std::strcmp(var, "cluster") == 0) {
     r.K = K;
     r.part = round_up((n + K - 1) / K, P);
     r.smem = r.part * eb;
     return r;
   }
   r.K = 0;
-  r.group_rows = std::max<int64_t>(1, (int64_t)(256ll << 20) / row_bytes);
+  const int64_t group_mb = env_int("T213_ROW_GROUP_MB") > 0 ? env_int("T213_ROW_GROUP_MB") : 64;
+  r.group_rows = std::max<int64_t>(1, (group_mb << 20) / row_bytes);
   return r;
 }
 
@@ -470,6 +491,40 @@ int count_col_gather(int64_t d3, int64_t m, int64_t n, int eb) {
 
 namespace {
 
+constexpr int kNoCluster = -1;  // launch_col_local_t: the cluster cannot be resident
+
+// Clusters of K CTAs that can be resident at once (0 if none fits), cached.
+int clusters_resident(const void *kern, int threads, int64_t smem, int K) {
+  static std::mutex mu;
+  static std::map<std::tuple<const void *, int64_t, int, int>, int> cache;
+  const int dev = dev_info().id;
+  const auto key = std::make_tuple(kern, smem, K, dev);
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(K * 8), 1, 1);
+  cfg.blockDim = dim3(threads, 1, 1);
+  cfg.dynamicSmemBytes = (size_t)smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = K;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int v = 0;
+  if (cudaOccupancyMaxActiveClusters(&v, kern, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    v = 0;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  cache[key] = v;
+  return v;
+}
+
 // k_col_local for one element size / access width / index width.
 template <int EB, int AW, typename U>
 int launch_col_local_t(const FnSpec &f, const LocalCfg &c, char *data, int64_t d3, int64_t m, int64_t n,
@@ -492,6 +547,11 @@ int launch_col_local_t(const FnSpec &f, const LocalCfg &c, char *data, int64_t d
     } else {
       auto kern = k_col_local<EB, AW, U, Off, Fs, Gs, true>;
       if ((status = prep_kernel(kern, c.smem, c.K))) return;
+      if (clusters_resident((const void *)kern, kGatherThreads, c.smem, c.K) < 1) {
+        // no GPC holds such a cluster: the caller takes another variant
+        status = kNoCluster;
+        return;
+      }
       const int64_t grid = persistent_grid(kern, kGatherThreads, c.smem, c.K, units);
       status = launch_k(kern, grid, kGatherThreads, c.smem, c.K, st, data, d3, (U)m, (U)n, (U)c.W, (U)c.WS,
                         n_strips, (U)c.H, (int)c.halo, off, F, G, stw);
@@ -536,8 +596,10 @@ int launch_col_gather(const FnSpec &f, char *data, int64_t d3, int64_t m, int64_
       return true;
     };
     dispatch_eb_aw(eb, lc.aw, run);
-    if (ls) ls->launches++;
-    return status;
+    if (status != kNoCluster) {
+      if (ls) ls->launches++;
+      return status;
+    }
   }
   ColCfg c = col_config(m, n, eb, data);
   const bool u32 = fits32(f, m, n);

@@ -386,17 +386,23 @@ void r2c_passes(Plan &P, int64_t m, int64_t n, bool skinny) {
   }
 }
 
+// Fraction of the copy rate a gather pass reaches, by variant, from B200
+// measurements: cluster-local column strips 0.5-0.64, staged column strips
+// 0.3-0.45, DSMEM-clustered columns about 0.25; staged rows 0.6-0.8.  Rows
+// longer than shared memory, gathered from a global scratch copy, about 0.17
+// (DSMEM-clustered rows 0.06); columns taller than a 16-CTA cluster, from a
+// scratch copy, about 0.06 (C2R on (344, 359054, 4) fp32).
 double gather_cost(const PassDesc &p, int eb) {
   if (p.type == PT_COL) {
     std::string d = describe_col_gather_fn(p.fn, p.m, p.n, eb, nullptr);
     if (d.find("[local") != std::string::npos) return 1 / 0.6;
-    if (d.find("scratch") != std::string::npos) return 1 / 0.2;
-    if (d.find("cluster=1 ") != std::string::npos) return 1 / 0.45;
-    return 1 / 0.3;
+    if (d.find("scratch") != std::string::npos) return 1 / 0.06;
+    if (d.find("cluster=1 ") != std::string::npos) return 1 / 0.4;
+    return 1 / 0.25;
   }
   std::string d = describe_row_gather(p.m, p.n, eb, nullptr);
-  if (d.find("scratch") != std::string::npos) return 1 / 0.25;
-  if (d.find("cluster") != std::string::npos) return 1 / 0.45;
+  if (d.find("scratch") != std::string::npos) return 1 / 0.17;
+  if (d.find("cluster") != std::string::npos) return 1 / 0.06;
   return 1 / 0.65;
 }
 
@@ -671,17 +677,20 @@ std::shared_ptr<Plan> get_plan(int64_t d1, int64_t d2, int64_t d3, int eb, int k
       cands.push_back({T213_PLAN_BANDS, tr, estimate_cost(T213_PLAN_BANDS, m, n, tr, eb, d3)});
       int64_t tc = pick_band_t_t(m, n, eb);
       cands.push_back({T213_PLAN_BANDS_T, tc, estimate_cost(T213_PLAN_BANDS_T, m, n, tc, eb, d3)});
-      // Catanzaro decomposition with the column height = min(d1,d2), as the
-      // reference's dispatcher chooses (src/transpose.cu:117-123)
-      {
+      // The Catanzaro decomposition both ways: the reference's dispatcher
+      // takes C2R when d1 >= d2, else R2C (src/transpose.cu:117-123); here
+      // both are costed, since which one keeps its rows inside shared
+      // memory decides the faster one for tall or wide slices.
+      for (int k : {T213_PLAN_C2R, T213_PLAN_R2C}) {
         Plan tmp;
         tmp.d1 = d1;
         tmp.d2 = d2;
         tmp.d3 = d3;
         tmp.eb = eb;
-        int k = (d1 >= d2) ? T213_PLAN_C2R : T213_PLAN_R2C;
         build_plan(tmp, k, 0);
-        cands.push_back({k, 0, plan_cost(tmp)});
+        // ties go to the reference's choice
+        const bool ref_choice = (k == T213_PLAN_C2R) == (d1 >= d2);
+        cands.push_back({k, 0, plan_cost(tmp) * (ref_choice ? 1.0 : 1.0001)});
       }
       std::sort(cands.begin(), cands.end(), [](const Cand &a, const Cand &b) { return a.est < b.est; });
       for (const Cand &c : cands) {

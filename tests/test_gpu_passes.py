@@ -17,8 +17,8 @@ pytestmark = pytest.mark.gpu
 
 # (d3, m, n): m rows, n columns per slice
 COL_SHAPES = [(2, 37, 53), (1, 900, 37), (2, 1537, 300), (1, 3000, 64), (1, 6151, 96), (2, 2048, 384),
-              (1, 4096, 30), (3, 1001, 1001), (1, 12000, 40)]
-ROW_SHAPES = [(2, 37, 53), (3, 97, 300), (1, 40, 7919), (2, 300, 2048), (1, 6, 60000)]
+              (1, 4096, 30), (3, 1001, 1001), (1, 12000, 40), (1, 40000, 16), (1, 100003, 8)]
+ROW_SHAPES = [(2, 37, 53), (3, 97, 300), (1, 40, 7919), (2, 300, 2048), (1, 6, 60000), (2, 5, 200003)]
 EBS = (4, 8, 16, 1, 2)
 
 
@@ -133,7 +133,8 @@ def test_row_shuffle(cuda, oracle, t213, shape, kind, eb):
     run_pass(cuda, oracle, t213, "row_shuffle", kind, params_for(kind, m, n, oracle), d3, m, n, eb)
 
 
-@pytest.mark.parametrize("variant,stage_kb", [("old", 0), ("pipe", 8), ("pipe", 24), ("pipe", 96)])
+@pytest.mark.parametrize("variant,stage_kb", [("old", 0), ("pipe", 8), ("pipe", 24), ("pipe", 96), ("cluster", 0),
+                                              ("scratch", 0)])
 @pytest.mark.parametrize("kind", (10, 12))
 def test_row_kernels(cuda, oracle, t213, monkeypatch, kind, variant, stage_kb):
     """The staged and the double-buffered row kernels, several unit sizes
@@ -141,7 +142,8 @@ def test_row_kernels(cuda, oracle, t213, monkeypatch, kind, variant, stage_kb):
     monkeypatch.setenv("T213_ROW_VARIANT", variant)
     if stage_kb:
         monkeypatch.setenv("T213_ROW_STAGE_KB", str(stage_kb))
-    for d3, m, n, eb in ((2, 97, 300, 4), (1, 301, 1001, 8), (3, 40, 7919, 8), (1, 1000, 33, 16), (2, 77, 513, 2)):
+    for d3, m, n, eb in ((2, 97, 300, 4), (1, 301, 1001, 8), (3, 40, 7919, 8), (1, 1000, 33, 16), (2, 77, 513, 2),
+                         (1, 4, 70001, 4), (2, 3, 30011, 8)):
         run_pass(cuda, oracle, t213, "row_shuffle", kind, params_for(kind, m, n, oracle), d3, m, n, eb)
 
 
