@@ -7,6 +7,14 @@
       place torch permute on the GPU.
   python -m 213transpose_b200.cli describe D1 D2 D3 ELEM_BYTES [--plan P]
   python -m 213transpose_b200.cli tune D1 D2 D3 ELEM_BYTES [--save FILE]
+  python -m 213transpose_b200.cli compare FILE_A FILE_B D1 D2 D3 TYPE_SIZE
+      compares two raw output files of the drivers (test_213inplace, gen_ans:
+      vol elements of TYPE_SIZE bytes, no header, as TensorUtil::write_file
+      writes them, src/tensor_util.cpp:69-72) element by element; prints the
+      mismatch count and the first mismatch as transposed-layout coordinates
+      (i2, i1, i3); exit status 1 on any difference.
+  python -m 213transpose_b200.cli dump FILE D1 D2 D3 TYPE_SIZE [--slice K] [--rows R]
+      prints slice K of a driver's output (transposed layout: d1 rows of d2).
 """
 from __future__ import annotations
 
@@ -15,9 +23,41 @@ import importlib
 import json
 
 
+def _raw(path, d1, d2, d3, ts):
+    import numpy as np
+    vol = d1 * d2 * d3
+    dt = {1: np.uint8, 2: np.uint16, 4: np.int32, 8: np.int64}.get(ts)
+    a = np.fromfile(path, dtype=np.uint8)
+    if a.size != vol * ts:
+        raise SystemExit(f"{path}: {a.size} bytes, expected {vol} elements of {ts} bytes ({vol * ts} bytes)")
+    return a.view(dt) if dt is not None else a.reshape(vol, ts)
+
+
+def compare(a_path, b_path, d1, d2, d3, ts) -> dict:
+    import numpy as np
+    a, b = _raw(a_path, d1, d2, d3, ts), _raw(b_path, d1, d2, d3, ts)
+    diff = (a != b) if a.ndim == 1 else (a != b).any(axis=1)
+    bad = np.flatnonzero(diff)
+    out = {"elements": int(d1 * d2 * d3), "mismatches": int(bad.size)}
+    if bad.size:
+        e = int(bad[0])  # transposed layout: i2 fastest, then i1, then i3
+        out["first"] = {"index": e, "i2": e % d2, "i1": (e // d2) % d1, "i3": e // (d1 * d2)}
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="213transpose_b200.cli")
     sub = ap.add_subparsers(dest="cmd", required=True)
+    pc = sub.add_parser("compare")
+    pc.add_argument("a")
+    pc.add_argument("b")
+    pd = sub.add_parser("dump")
+    pd.add_argument("file")
+    for p in (pc, pd):
+        for name in ("d1", "d2", "d3", "type_size"):
+            p.add_argument(name, type=int)
+    pd.add_argument("--slice", type=int, default=0)
+    pd.add_argument("--rows", type=int, default=8)
     for name in ("run", "describe", "tune"):
         p = sub.add_parser(name)
         p.add_argument("d1", type=int)
@@ -32,6 +72,17 @@ def main(argv=None):
         if name == "tune":
             p.add_argument("--save", default=None)
     a = ap.parse_args(argv)
+    if a.cmd == "compare":
+        r = compare(a.a, a.b, a.d1, a.d2, a.d3, a.type_size)
+        print(json.dumps(r))
+        raise SystemExit(1 if r["mismatches"] else 0)
+    if a.cmd == "dump":
+        x = _raw(a.file, a.d1, a.d2, a.d3, a.type_size)
+        per = a.d1 * a.d2
+        sl = x[a.slice * per:(a.slice + 1) * per]
+        for r in range(min(a.rows, a.d1)):
+            print(" ".join(str(v) for v in sl[r * a.d2:(r + 1) * a.d2][:16]) + (" ..." if a.d2 > 16 else ""))
+        return
     t213 = importlib.import_module("213transpose_b200")
     if a.cmd == "describe":
         print(t213.describe(a.d1, a.d2, a.d3, a.elem_bytes, a.plan, a.t))
