@@ -74,6 +74,7 @@ _SIGS = {
     "t213_col_shuffle": ([_i32, _pi64, _i32, _vp, _i64, _i64, _i64, _i32, _vp], ctypes.c_int),
     "t213_scatter_permute": ([_i32, _pi64, _i32, _vp, _i64, _i64, _i64, _i32, _vp], ctypes.c_int),
     "t213_transpose_host": ([_vp, _i64, _i64, _i64, _i32, _vp], ctypes.c_int),
+    "t213_permute": ([_vp, _i32, _pi64, ctypes.POINTER(_i32), _i32, _vp], ctypes.c_int),
     "t213_plan_describe": ([_i64, _i64, _i64, _i32, _i32, _i64, ctypes.c_char_p, _sz], ctypes.c_int),
     "t213_plan_launches": ([_i64, _i64, _i64, _i32, _i32, _i64, ctypes.POINTER(_i32)], ctypes.c_int),
     "t213_pass_timing_enable": ([_i32], ctypes.c_int),

@@ -159,6 +159,19 @@ def transpose_with_plan(data, d1, d2, d3, plan, t=0, *, elem_bytes=None, stream=
     check(lib().t213_transpose_with_plan(p, int(d1), int(d2), int(d3), eb, kind, int(t), st))
 
 
+def permute(data, dims, perm, *, elem_bytes=None, stream=None):
+    """In-place permutation of the axes of a rank-N array: dims[0] fastest,
+    output axis j is input axis perm[j] (the reference's TensorUtil model,
+    src/tensor_util.cpp:7-23,79-92); at most rank-1 213 transposes."""
+    p, eb, st = _resolve(data, elem_bytes, stream)
+    n = len(dims)
+    if len(perm) != n:
+        raise ValueError("dims and perm must have the same length")
+    cd = (ctypes.c_int64 * max(1, n))(*[int(v) for v in dims])
+    cp = (ctypes.c_int32 * max(1, n))(*[int(v) for v in perm])
+    check(lib().t213_permute(p, n, cd, cp, eb, st))
+
+
 def transpose_host(data, d1, d2, d3, *, elem_bytes=None, stream=None):
     """End-to-end transpose of a host buffer (torch CPU tensor, numpy array or
     raw pointer): copy in, transpose, copy out.  Synchronous."""

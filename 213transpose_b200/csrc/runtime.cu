@@ -1002,6 +1002,84 @@ int t213_transpose_with_plan(void *data, int64_t d1, int64_t d2, int64_t d3, int
   return run_shape(data, d1, d2, d3, elem_bytes, plan_kind, t, (cudaStream_t)stream, 0);
 }
 
+int t213_permute(void *data, int32_t rank, const int64_t *dims, const int32_t *perm, int32_t elem_bytes,
+                 t213_stream_t stream) {
+  if (rank < 0 || rank > 32 || (rank > 0 && (!dims || !perm))) {
+    set_error("t213_permute: rank must be 0..32 with dims and perm given");
+    return T213_ERR_INVALID_ARGUMENT;
+  }
+  std::vector<int> seen(rank, 0);
+  double vol = 1;
+  for (int i = 0; i < rank; i++) {
+    if (dims[i] < 0 || perm[i] < 0 || perm[i] >= rank || seen[perm[i]]++) {
+      set_error("t213_permute: dims must be >= 0 and perm a permutation of 0..rank-1");
+      return T213_ERR_INVALID_ARGUMENT;
+    }
+    vol *= (double)dims[i];
+  }
+  if (vol * elem_bytes >= 9.0e18) {
+    set_error("tensor too large");
+    return T213_ERR_INVALID_ARGUMENT;
+  }
+  const int rc0 = check_args(data, vol > 0 ? 1 : 0, 1, 1, elem_bytes);  // element size, NULL, alignment
+  if (rc0) return rc0;
+  if (vol == 0 || rank < 2) return T213_OK;
+  // Leading axes the permutation keeps in place become part of the element:
+  // up to 16 bytes the 213 plans move it as one element; from 64 bytes on,
+  // a 213 step of such elements is a single segment-cycle pass (one read and
+  // one write of the tensor) as long as its cycle table stays small.
+  const double total_bytes = vol * elem_bytes;
+  int64_t E = elem_bytes;
+  int q0 = 0;
+  while (q0 < rank - 1 && perm[q0] == q0) {
+    const int64_t E2 = E * dims[q0];
+    const bool small = E2 <= 16 && (E2 & (E2 - 1)) == 0;
+    const bool seg = E2 >= 64 && total_bytes / (double)E2 <= 4.0e6;
+    if (!small && !seg) break;
+    E = E2;
+    q0++;
+  }
+  // cur[q]: the input axis now at position q (fastest first) among axes
+  // q0..rank-1.  For k from the slowest position down, bring perm[k] to
+  // position k by rotating the prefix [q0, k]: the group [q0, p] (ending with
+  // that axis) moves behind the group [p+1, k], which is one 213 transpose
+  // with d1 = the first group's volume, d2 = the second's and d3 = everything
+  // slower.
+  std::vector<int> cur(rank);
+  for (int i = 0; i < rank; i++) cur[i] = i;
+  for (int k = rank - 1; k > q0; k--) {
+    int p = q0;
+    while (cur[p] != perm[k]) p++;
+    if (p == k) continue;
+    int64_t g1 = 1, g2 = 1, g3 = 1;
+    for (int q = q0; q <= p; q++) g1 *= dims[cur[q]];
+    for (int q = p + 1; q <= k; q++) g2 *= dims[cur[q]];
+    for (int q = k + 1; q < rank; q++) g3 *= dims[cur[q]];
+    int rc;
+    if (E <= 16) {
+      rc = run_shape(data, g1, g2, g3, (int32_t)E, T213_PLAN_AUTO, 0, (cudaStream_t)stream, 0);
+    } else if (g1 == 1 || g2 == 1) {
+      rc = T213_OK;  // the memory layout does not change
+    } else {
+      // segments of E bytes: [g2][g1] -> [g1][g2] in each of the g3 slices
+      PermSpec ps;
+      ps.kind = 0;
+      ps.A = g2;
+      ps.Mid = 1;
+      ps.C = g1;
+      ps.S = g1 * g2;
+      rc = T213_OK;
+      auto ct = get_cycle_table(ps, items_per_chunk(E, g3), &rc);
+      if (!ct) return rc;
+      if (ct->n_chunks > 0)
+        rc = launch_seg_cycles(*ct, (char *)data, g3, g1 * g2 * E, E, (cudaStream_t)stream, nullptr, nullptr, 0);
+    }
+    if (rc) return rc;
+    std::rotate(cur.begin() + q0, cur.begin() + p + 1, cur.begin() + k + 1);
+  }
+  return T213_OK;
+}
+
 int t213_c2r_transpose(void *data, int64_t d1, int64_t d2, int64_t d3, int32_t elem_bytes, t213_stream_t stream) {
   return run_shape(data, d1, d2, d3, elem_bytes, 0, 0, (cudaStream_t)stream, 1);
 }

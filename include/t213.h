@@ -102,6 +102,17 @@ int t213_transpose(void *data, int64_t d1, int64_t d2, int64_t d3, int32_t elem_
 int t213_transpose_with_plan(void *data, int64_t d1, int64_t d2, int64_t d3, int32_t elem_bytes,
                              int32_t plan_kind, int64_t t, t213_stream_t stream);
 
+/* In-place permutation of the axes of a rank-N tensor, as a sequence of at
+ * most N-1 in-place 213 transposes of grouped axes.  The convention is the
+ * reference's rank-N model (TensorUtil, src/tensor_util.cpp:7-23,79-92):
+ * dims[0] is the fastest axis, and output axis j (fastest first) is input
+ * axis perm[j], so perm = {1, 0, 2} is the 213 transpose.  The reference's
+ * GPU library has no rank-N call (its TensorUtil::seq_tt is an out-of-place
+ * CPU gather); this entry point is the in-place GPU counterpart.  rank <= 32;
+ * perm must be a permutation of 0..rank-1.  Asynchronous on `stream`. */
+int t213_permute(void *data, int32_t rank, const int64_t *dims, const int32_t *perm, int32_t elem_bytes,
+                 t213_stream_t stream);
+
 /* Replaces template<T> void inplace::c2r::transpose(T*, int d1, int d2, int d3)
  * (include/transpose.h:5-9, src/transpose.cu:30-47): the slice is a d2 x d1
  * row-major matrix (m = d2 rows, n = d1 columns) transposed to d1 x d2 by

@@ -15,6 +15,14 @@ def test_registered_and_meta_shape():
     assert y is x and tuple(x.shape) == (5, 4, 3) and x.is_contiguous()
 
 
+def test_permute_meta_shape():
+    x = torch.empty(2, 3, 4, 5, device="meta")
+    torch.ops.t213.permute_(x, [3, 1, 0, 2])
+    assert tuple(x.shape) == (5, 3, 2, 4) and x.is_contiguous()
+    with pytest.raises(Exception):
+        torch.ops.t213.permute_(torch.empty(2, 3, device="meta"), [0, 0])
+
+
 def test_refuses_cpu_tensors():
     with pytest.raises(RuntimeError):
         torch.ops.t213.transpose_(torch.zeros(2, 3, 4))
