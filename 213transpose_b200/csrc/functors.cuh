@@ -152,6 +152,14 @@ struct RowC2RShuffle {  // equations.h:12-54 (and the 64-bit long_shuffle, skinn
     k = (U)kk;
   }
   T213_HD U operator()(U i, U j) const {
+    if (c.get() == 1) {
+      // coprime m, n: f = j + i(n-1) (i < m always satisfies the low test), so
+      // f mod n = (j - i) mod n and s = k * (j - i) mod n, with k < b = n
+      const U nn = n.get();
+      const U im = i < nn ? i : n.mod(i);
+      const U d = j >= im ? j - im : j + nn - im;
+      return n.mod(k * d);
+    }
     U jc = c.mod(j);
     // i - (j mod c) <= m - c, evaluated without unsigned wrap
     bool low = i + c.get() <= m + jc;
@@ -169,6 +177,7 @@ struct RowR2CShuffle {  // equations.h:178-194
   RowR2CShuffle() = default;
   __host__ RowR2CShuffle(int64_t m_, int64_t n_, int64_t c_) : m(m_), n(n_), b(n_ / (c_ > 0 ? c_ : 1)) {}
   T213_HD U operator()(U i, U j) const {
+    if (b.get() == n.get()) return n.mod(i + j * m.get());  // c = 1: j / b = 0 and i < m
     U r = m.mod(b.div(j) + i) + j * m.get();
     return n.mod(r);
   }
