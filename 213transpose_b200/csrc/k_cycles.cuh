@@ -132,12 +132,11 @@ __global__ void __launch_bounds__(kCycleThreads)
 // ---------------------------------------------------------------------------
 constexpr int kBulkRing = 6;
 
-template <typename P, typename U>
+template <typename P, typename U, int NB = kBulkRing>
 __global__ void __launch_bounds__(32)
     k_seg_cycles_bulk(char *__restrict__ data, int64_t slice_bytes, int64_t d3, int64_t seg_bytes,
                       int64_t piece_bytes, int64_t pieces, const Chunk *__restrict__ chunks, int64_t n_chunks,
                       const char *__restrict__ carry, P dst, int *status) {
-  constexpr int NB = kBulkRing;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
   char *buf = reinterpret_cast<char *>(smem_raw) + 128;

@@ -6,6 +6,7 @@
 // spreads over the whole GPU.  Tables are cached per permutation and device
 // and uploaded once; they are the "precomputed cycle leaders" of the pass.
 #include <algorithm>
+#include <cstdlib>
 #include <cstdio>
 #include <list>
 #include <map>
@@ -319,10 +320,15 @@ int launch_seg_cycles(const CycleTable &ct, char *data, int64_t d3, int64_t slic
   }
   bool ok = false;
   if (aw == 16 && seg_bytes >= 1024) {
-    // TMA bulk walker: pieces of up to 16 KB, a ring of kBulkRing buffers
-    const int64_t piece = std::min<int64_t>(seg_bytes, 16 * 1024);
+    // TMA bulk walker: pieces of up to 16 KB (T213_SEG_PIECE_KB), a ring of
+    // 6 buffers (T213_SEG_RING=10 for 10)
+    const char *pv = std::getenv("T213_SEG_PIECE_KB");
+    const int64_t piece_cap = (pv && std::atoi(pv) > 0 ? std::atoi(pv) : 16) * 1024;
+    const char *rv = std::getenv("T213_SEG_RING");
+    const int ring = (rv && std::atoi(rv) == 10) ? 10 : kBulkRing;
+    const int64_t piece = std::min<int64_t>(seg_bytes, piece_cap);
     const int64_t npieces = (seg_bytes + piece - 1) / piece;
-    const int64_t smem = 128 + (int64_t)kBulkRing * piece;
+    const int64_t smem = 128 + (int64_t)ring * piece;
     int *stw = device_status_word(&status);
     if (!stw) return status;
     if (ct.n_carry > 0) {
@@ -338,7 +344,7 @@ int launch_seg_cycles(const CycleTable &ct, char *data, int64_t d3, int64_t slic
       using U = decltype(UT);
       return with_perm<U>(ct.spec, [&](auto dst) -> bool {
         using P = decltype(dst);
-        auto kern = k_seg_cycles_bulk<P, U>;
+        auto kern = ring == 10 ? k_seg_cycles_bulk<P, U, 10> : k_seg_cycles_bulk<P, U, kBulkRing>;
         if (!kernel_attr_once((const void *)kern, smem, 1)) {
           status = cuda_status(cudaGetLastError(), "cudaFuncSetAttribute(bulk walker)");
           return true;
