@@ -89,3 +89,14 @@ def test_config3_skinny_every_applicable_plan(cuda, oracle, t213, plan):
         dev = to_device(cuda, x)
         t213.transpose_with_plan(dev, d1, d2, d3, plan, elem_bytes=eb)
         assert np.array_equal(from_device(dev), want), (plan, d1, d2, d3)
+
+
+@pytest.mark.parametrize("shape", [(1 << 16, (1 << 15) + 1, 1, 4), (46341, 46345, 1, 4)],
+                         ids=["65536x32769", "46341x46345"])
+def test_more_than_2p31_elements(cuda, t213, shape):
+    """Tensors of more than 2^31 elements (8.6 GB fp32): the 64-bit index
+    paths of the functors, checked against torch's out-of-place permute on
+    the device and by the round trip."""
+    d1, d2, d3, eb = shape
+    assert d1 * d2 * d3 > (1 << 31)
+    _device_property_check(cuda, t213, d1, d2, d3, eb, seed=7)
