@@ -100,7 +100,7 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 }
 
 // Tiled TMA load of one box of a 3-D tensor map into shared memory
-// (cp.async.bulk.tensor, no multicast), completion counted on bar.  The x
+// (cp.async.bulk.tensor into this CTA's own buffer), completion counted on bar.  The x
 // coordinate is in elements of the map's data type and must be a multiple of
 // 16 bytes.
 __device__ __forceinline__ void tma_load_3d(void *dst_smem, const void *tmap, int32_t x, int32_t y, int32_t z,
