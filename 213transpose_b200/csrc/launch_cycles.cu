@@ -1,9 +1,9 @@
 // Cycle tables (host) and the launch of the segment-cycle walkers.
 //
 // The host lists every non-trivial cycle of a segment permutation with a
-// visited bitmap (O(S) functor evaluations with the device's own arithmetic),
-// then cuts cycles longer than a target length into chunks so the walk
-// spreads over the whole GPU.  Tables are cached per permutation and device
+// visited bitmap (O(S) functor evaluations with the device's own arithmetic)
+// and, in the same walk, cuts cycles longer than a target length into chunks
+// so the walk spreads over the whole GPU.  Tables are cached per permutation and device
 // and uploaded once; they are the "precomputed cycle leaders" of the pass.
 #include <algorithm>
 #include <cstdlib>
@@ -69,59 +69,54 @@ void flush_deferred_frees() {
 
 namespace {
 
-struct Cyc {
-  int64_t start, len;
-};
-
+// One walk over the positions lists every non-trivial cycle and cuts it into
+// chunks as it goes: the chunk length Lc is fixed up front from S (an upper
+// bound of the moved positions) so that about 8 walker items exist per
+// resident walker team, and the walk records the position at every Lc-th
+// step of a cycle.  A cycle of at most Lc moves is one whole chunk (its walker
+// reads the start itself); a longer one becomes chunks of Lc moves (the last
+// one shorter) whose starts are saved to carry slots before the walkers run.
 template <typename P>
-int walk_cycles(const P &dst, int64_t S, std::vector<Cyc> &cycles, int64_t &moved, int64_t &max_len) {
+int walk_and_chunk(const P &dst, int64_t S, int64_t items_per_chunk, std::vector<Chunk> &chunks,
+                   std::vector<CarryItem> &carries, int64_t &n_cycles, int64_t &moved, int64_t &max_len) {
+  const DevInfo &d = dev_info();
+  const int64_t resident_teams = (int64_t)d.sms * 8;
+  const int64_t target_chunks = std::max<int64_t>(1, 8 * resident_teams / std::max<int64_t>(1, items_per_chunk));
+  const int64_t Lc = std::max<int64_t>(16, (S + target_chunks - 1) / target_chunks);
   std::vector<uint64_t> seen((size_t)((S + 63) / 64), 0);
-  moved = 0;
-  max_len = 0;
+  std::vector<int64_t> marks;
+  n_cycles = moved = max_len = 0;
   for (int64_t p = 0; p < S; p++) {
     if (seen[p >> 6] >> (p & 63) & 1) continue;
-    int64_t x = p, len = 0;
+    marks.clear();
+    int64_t x = p, len = 0, k = 0;
     do {
       if (x < 0 || x >= S || (seen[x >> 6] >> (x & 63) & 1)) {
         set_error("segment map is not a permutation of its index range");
         return T213_ERR_INVALID_ARGUMENT;
       }
       seen[x >> 6] |= 1ull << (x & 63);
+      if (k == 0) {
+        marks.push_back(x);
+        k = Lc;
+      }
+      k--;
       x = (int64_t)dst(x);
       len++;
     } while (x != p);
-    if (len > 1) {
-      cycles.push_back({p, len});
-      moved += len;
-      max_len = std::max(max_len, len);
-    }
-  }
-  return T213_OK;
-}
-
-template <typename P>
-int chunk_cycles(const P &dst, const std::vector<Cyc> &cycles, int64_t moved, int64_t items_per_chunk,
-                 std::vector<Chunk> &chunks, std::vector<CarryItem> &carries) {
-  const DevInfo &d = dev_info();
-  // aim for ~8 walker items per resident team
-  const int64_t resident_teams = (int64_t)d.sms * 8;
-  const int64_t target_chunks = std::max<int64_t>(1, 8 * resident_teams / std::max<int64_t>(1, items_per_chunk));
-  const int64_t Lc = std::max<int64_t>(16, (moved + target_chunks - 1) / target_chunks);
-  for (const Cyc &c : cycles) {
-    if (c.len <= Lc) {
-      chunks.push_back({c.start, c.len, -1});
+    if (len < 2) continue;
+    n_cycles++;
+    moved += len;
+    max_len = std::max(max_len, len);
+    if (len <= Lc) {
+      chunks.push_back({p, len, -1});
       continue;
     }
-    const int64_t nch = (c.len + Lc - 1) / Lc;
-    const int64_t each = (c.len + nch - 1) / nch;
-    int64_t x = c.start, done = 0;
-    while (done < c.len) {
-      const int64_t l = std::min(each, c.len - done);
+    for (size_t i = 0; i < marks.size(); i++) {
+      const int64_t l = std::min<int64_t>(Lc, len - (int64_t)i * Lc);
       const int64_t slot = (int64_t)carries.size();
-      carries.push_back({x, slot});
-      chunks.push_back({x, l, slot});
-      for (int64_t s = 0; s < l; s++) x = (int64_t)dst(x);
-      done += l;
+      carries.push_back({marks[i], slot});
+      chunks.push_back({marks[i], l, slot});
     }
   }
   std::stable_sort(chunks.begin(), chunks.end(), [](const Chunk &a, const Chunk &b) { return a.len > b.len; });
@@ -187,15 +182,13 @@ std::shared_ptr<CycleTable> get_cycle_table(const PermSpec &p, int64_t items_per
       }
     }
   }
-  std::vector<Cyc> cycles;
   std::vector<Chunk> chunks;
   std::vector<CarryItem> carries;
-  int64_t moved = 0, max_len = 0;
+  int64_t moved = 0, max_len = 0, n_cycles = 0;
   int rc = T213_OK;
   bool ok;
   auto build = [&](auto fn) -> bool {
-    rc = walk_cycles(fn, p.S, cycles, moved, max_len);
-    if (rc == T213_OK) rc = chunk_cycles(fn, cycles, moved, items_per_chunk, chunks, carries);
+    rc = walk_and_chunk(fn, p.S, items_per_chunk, chunks, carries, n_cycles, moved, max_len);
     return true;
   };
   if (perm_fits32(p))
@@ -217,7 +210,7 @@ std::shared_ptr<CycleTable> get_cycle_table(const PermSpec &p, int64_t items_per
   ct->n_chunks = (int64_t)chunks.size();
   ct->n_carry = (int64_t)carries.size();
   ct->moved = moved;
-  ct->n_cycles = (int64_t)cycles.size();
+  ct->n_cycles = n_cycles;
   ct->max_len = max_len;
   ct->h_chunks.assign((const char *)chunks.data(), (const char *)(chunks.data() + chunks.size()));
   ct->h_carry_items.assign((const char *)carries.data(), (const char *)(carries.data() + carries.size()));
