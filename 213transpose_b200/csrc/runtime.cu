@@ -301,8 +301,8 @@ int add_seg_pass(Plan &P, const PermSpec &ps, int64_t seg_bytes, bool skip_ident
 double seg_eff(int64_t seg_bytes) {
   if (seg_bytes >= 4096) return 0.88;
   if (seg_bytes >= 1024) return 0.8;
-  if (seg_bytes >= 512) return 0.55;
-  if (seg_bytes >= 256) return 0.4;
+  if (seg_bytes >= 512) return 0.65;  // bulk walker when 16-byte aligned: 0.72 at 704 B
+  if (seg_bytes >= 256) return 0.5;   // 0.61 at 480 B
   if (seg_bytes >= 128) return 0.3;
   if (seg_bytes >= 64) return 0.18;
   return 0.08;
