@@ -123,34 +123,47 @@ def ncu_traffic(pass_name: str):
         return None
 
 
-def init_dist(n_gpus):
+def init_dist(n_gpus, backend="nccl"):
+    """One process per GPU under torchrun (RANK/LOCAL_RANK/WORLD_SIZE/MASTER_*
+    from the environment); (None, 0, 1, 0) for a single process.  The CPU
+    tests use backend "gloo"."""
     if n_gpus <= 1 or "RANK" not in os.environ:
         return None, 0, 1, 0
     import torch
     import torch.distributed as dist
     import datetime
     local = int(os.environ.get("LOCAL_RANK", 0))
-    torch.cuda.set_device(local)
-    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                            device_id=torch.device("cuda", local))
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return dist, dist.get_rank(), dist.get_world_size(), local
 
 
-def max_over_ranks(dist, value: float) -> float:
+def max_over_ranks(dist, value: float, device="cuda") -> float:
     if dist is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
 
-def barrier(dist):
+def barrier(dist, device="cuda"):
     if dist is not None:
         import torch
-        t = torch.zeros(1, device="cuda")
+        t = torch.zeros(1, device=device)
         dist.all_reduce(t)
-        torch.cuda.synchronize()
+        if device == "cuda":
+            torch.cuda.synchronize()
+
+
+def whole_job_gbps(world: int, nbytes: int, steps: int, ms_max: float) -> float:
+    """Effective 2 x bytes / time of all ranks' replicas, timed as the max
+    over ranks (each rank transposes its own tensor of nbytes per step)."""
+    return world * 2 * nbytes * steps / (ms_max * 1e-3) / 1e9
 
 
 # ------------------------------------------------------------ our arm --------
@@ -262,7 +275,7 @@ def run_ours(args):
         serving = serving_section(t213, torch)
 
     if rank == 0:
-        value = world * 2 * nbytes * args.steps / (ms_max * 1e-3) / 1e9
+        value = whole_job_gbps(world, nbytes, args.steps, ms_max)
         n_passes = len(per)
         line = {
             "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
