@@ -83,6 +83,14 @@ CONFIG_PLANS = [
 ]
 
 
+@pytest.mark.parametrize("shape", [(7919, 6151, 2, 8), (8192, 6143, 2, 4), (6151, 7919, 2, 8)])
+def test_tall_column_passes_use_the_cluster_local_kernel(t213, shape):
+    """Coprime configurations take the cluster-local column gather with
+    128-byte strips."""
+    desc = t213.describe(*shape)
+    assert "[local W=" in desc and "cluster=8" in desc, desc
+
+
 @pytest.mark.parametrize("shape,prefix", CONFIG_PLANS, ids=lambda v: str(v))
 def test_planner_choices(t213, shape, prefix):
     desc = t213.describe(*shape)
