@@ -86,6 +86,7 @@ _SIGS = {
     "t213_batch_execute": ([_vp, _vp], ctypes.c_int),
     "t213_batch_status": ([_vp, _vp], ctypes.c_int),
     "t213_batch_describe": ([_vp, ctypes.c_char_p, _sz], ctypes.c_int),
+    "t213_batch_debug_stall": ([_vp, _i64, _i32], ctypes.c_int),
     "t213_batch_destroy": ([_vp], ctypes.c_int),
     "t213_transpose_looped": ([ctypes.POINTER(TensorDesc), _i32, _vp], ctypes.c_int),
     "t213_batch_tune": ([ctypes.POINTER(TensorDesc), _i32, _vp], ctypes.c_int),

@@ -87,20 +87,24 @@ def build(jobs: int | None = None, force: bool = False, drivers: bool = True) ->
 
 
 def build_drivers() -> None:
-    """test_213inplace and gen_ans with the reference's argv and output format,
-    linked against lib/libinplacett.a."""
+    """The reference's two drivers with its argv and output format:
+    test_213inplace (the GPU path, linked against lib/libinplacett.a) and
+    gen_ans (the host answer generator, plain C++ with no GPU code)."""
     os.makedirs(BINDIR, exist_ok=True)
     drv = os.path.join(PKG, "drivers")
     if not os.path.isdir(drv):
         return
-    for name in ("test_213inplace", "gen_ans"):
-        src = os.path.join(drv, name + ".cu")
+    for name, src_name in (("test_213inplace", "test_213inplace.cu"), ("gen_ans", "gen_ans.cpp")):
+        src = os.path.join(drv, src_name)
         if not os.path.exists(src):
             continue
         out = os.path.join(BINDIR, name)
         if os.path.exists(out) and os.path.getmtime(out) > max(os.path.getmtime(src), os.path.getmtime(STATIC)):
             continue
-        cmd = [nvcc()] + NVCC_FLAGS + [src, "-o", out, "-L" + LIBDIR, "-linplacett"]
+        if src.endswith(".cpp"):
+            cmd = ["g++", "-O3", "-std=c++17", src, "-o", out]
+        else:
+            cmd = [nvcc()] + NVCC_FLAGS + [src, "-o", out, "-L" + LIBDIR, "-linplacett"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"driver build failed for {name}:\n{r.stdout}\n{r.stderr}")

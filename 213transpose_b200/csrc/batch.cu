@@ -42,6 +42,9 @@ struct t213_batch_st {
   cudaEvent_t fork = nullptr, join = nullptr;
   std::string desc;
   int64_t total_bytes = 0;
+  // limit of every dependency wait of the persistent kernel (nanoseconds of
+  // %globaltimer); lowered only by t213_batch_debug_stall
+  uint64_t wait_ns = kWaitNs;
 };
 
 namespace {
@@ -473,7 +476,8 @@ static int batch_enqueue(t213_batch B, cudaStream_t st) {
   if (e != cudaSuccess) return cuda_status(e, "batch counters reset");
   if (!B->h_items.empty()) {
     k_batch<<<B->grid, kBatchThreads, (size_t)(kBatchSmem + kBatchBarBytes), st>>>(
-        B->d_passes, B->d_items, (int64_t)B->h_items.size(), B->d_ctrs, B->d_ctrs + B->n_ctrs, B->d_status);
+        B->d_passes, B->d_items, (int64_t)B->h_items.size(), B->d_ctrs, B->d_ctrs + B->n_ctrs, B->d_status,
+        B->wait_ns);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e, "k_batch launch");
   }
@@ -579,6 +583,31 @@ int t213_batch_tune(const t213_tensor_desc *tensors, int32_t count, t213_stream_
   cudaStreamSynchronize((cudaStream_t)stream);
   cudaFree(scratch);
   return rc;
+}
+
+int t213_batch_debug_stall(t213_batch B, int64_t wait_ns, int32_t stall_pass) {
+  if (!B || wait_ns <= 0) return T213_ERR_INVALID_ARGUMENT;
+  if (stall_pass < 0)
+    for (size_t i = 0; i < B->h_passes.size() && stall_pass < 0; i++)
+      if (B->h_passes[i].dep_ctr >= 0) stall_pass = (int32_t)i;
+  if (stall_pass < 0 || stall_pass >= (int32_t)B->h_passes.size() || B->h_passes[stall_pass].dep_ctr < 0) {
+    set_error("t213_batch_debug_stall: no pass with a dependency to stall");
+    return T213_ERR_INVALID_ARGUMENT;
+  }
+  cudaError_t e = cudaDeviceSynchronize();  // no execute may still read the pass table
+  if (e != cudaSuccess) return cuda_status(e, "t213_batch_debug_stall");
+  // one item more than the predecessor pass has: its counter never gets there
+  B->h_passes[stall_pass].dep_target += 1;
+  e = cudaMemcpy(B->d_passes + stall_pass, &B->h_passes[stall_pass], sizeof(BPass), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_status(e, "t213_batch_debug_stall upload");
+  B->wait_ns = (uint64_t)wait_ns;
+  // the captured graph holds the old launch parameters
+  if (B->exec) cudaGraphExecDestroy(B->exec);
+  if (B->graph) cudaGraphDestroy(B->graph);
+  B->exec = nullptr;
+  B->graph = nullptr;
+  B->graph_stream = nullptr;
+  return T213_OK;
 }
 
 int t213_batch_describe(t213_batch B, char *buf, size_t buflen) {

@@ -9,7 +9,8 @@
 // tensor has completed all its items (a per-pass counter), runs the item, and
 // counts it done.  Every item an item waits on sits earlier in the queue and
 // was claimed by a running CTA, so the waits always end; they are bounded
-// anyway (T213_ERR_TIMEOUT in *status, then the CTA leaves).
+// anyway (wait_ns of the global timer, 2 s unless a test lowers it; then
+// T213_ERR_TIMEOUT in *status and the CTA leaves).
 //
 // Unit executors:
 //   TILE   tile pairs of t x t block transposes (16-byte vectors when possible)
@@ -665,7 +666,7 @@ __device__ bool bx_dispatch(const BPass &P, const AnyFn<U> &f, int64_t u0, int64
 
 __global__ void __launch_bounds__(kBatchThreads, 1)
     k_batch(const BPass *__restrict__ passes, const BItem *__restrict__ items, int64_t n_items,
-            unsigned long long *ctrs, unsigned long long *head, int *status) {
+            unsigned long long *ctrs, unsigned long long *head, int *status, uint64_t wait_ns) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
   unsigned char *dyn = smem_raw + kBatchBarBytes;
@@ -694,7 +695,7 @@ __global__ void __launch_bounds__(kBatchThreads, 1)
       uint64_t t0 = 0;
       while (*dc < (unsigned long long)P.dep_target) {
         if (polls == 0) t0 = global_ns();
-        if (++polls > kWaitLimit || ((polls & 15) == 0 && global_ns() - t0 > kWaitNs)) {
+        if (++polls > kWaitLimit || ((polls & 15) == 0 && global_ns() - t0 > wait_ns)) {
           s_fail = 1;
           break;
         }

@@ -7,10 +7,13 @@
 // kernel are stream-ordered, so the next group's copy cannot overwrite the
 // scratch before the previous gather has read it.
 //
-// No device memory is allocated: the scratch lives in the library's module
-// (the driver reserves it when the module is loaded), its address is looked
-// up once per device, and the launch needs no dynamic shared memory and no
-// cached occupancy query.
+// No device memory is allocated by a call: the scratch lives in this file's
+// module, whose 32 MiB the CUDA driver reserves on a device when it loads the
+// module there.  With CUDA's default lazy module loading that happens at the
+// first use on the device -- in set-up, where the scratch address is looked
+// up -- so the first call on a device (an empty call is enough) must come
+// before the caller's own allocator has filled the device.  After that the
+// launch needs no dynamic shared memory and no cached occupancy query.
 #include <mutex>
 
 #include "../../include/t213_noalloc.h"
@@ -120,20 +123,12 @@ extern "C" int t213_row_shuffle_noalloc(int32_t fn_kind, const int64_t *fn_param
     set_error("row shuffler parameters must be (m=d2, n=d1, c>0, k)");
     return T213_ERR_INVALID_ARGUMENT;
   }
-  if (d1 == 0 || d2 == 0 || d3 == 0) return T213_OK;
-  if (!data) {
-    set_error("data is NULL");
-    return T213_ERR_INVALID_ARGUMENT;
-  }
-  if (((uintptr_t)data) % (uintptr_t)std::min(eb, 16)) {
-    set_error("data is not aligned to its element size");
-    return T213_ERR_INVALID_ARGUMENT;
-  }
   const int64_t row_bytes = n * eb;
   if (row_bytes > T213_NOALLOC_SCRATCH_BYTES) {
     set_error("a row is longer than the 32 MiB no-alloc scratch (d1 * elem_bytes > T213_NOALLOC_SCRATCH_BYTES)");
     return T213_ERR_UNSUPPORTED;
   }
+  // set-up first, so that an empty call reserves the scratch on this device
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_status(e, "cudaGetDevice");
@@ -144,6 +139,15 @@ extern "C" int t213_row_shuffle_noalloc(int32_t fn_kind, const int64_t *fn_param
   NoallocDevice *D = nullptr;
   int rc = setup(dev, &D);
   if (rc) return rc;
+  if (d1 == 0 || d2 == 0 || d3 == 0) return T213_OK;
+  if (!data) {
+    set_error("data is NULL");
+    return T213_ERR_INVALID_ARGUMENT;
+  }
+  if (((uintptr_t)data) % (uintptr_t)std::min(eb, 16)) {
+    set_error("data is not aligned to its element size");
+    return T213_ERR_INVALID_ARGUMENT;
+  }
 
   cudaStream_t st = (cudaStream_t)stream;
   const int aw = (eb >= 16 || (eb >= 4 && (((uintptr_t)data | (uint64_t)row_bytes) & 15) == 0)) ? 16 : eb;

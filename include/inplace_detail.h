@@ -9,6 +9,8 @@
  */
 #pragma once
 
+#include <stdint.h>
+
 #include <stdexcept>
 #include <string>
 
@@ -20,7 +22,7 @@ namespace detail {
 
 struct functor_desc {
   int kind;
-  long long p[4];
+  int64_t p[4];  /* the constructor's arguments, in the reference's order */
   int np;
 };
 
@@ -92,7 +94,7 @@ typedef c2r::postpermuter scatter_prepermuter;
 /* include/rotate.h:6-7 */
 template <typename F, typename T>
 void rotate(F f, int d3, int d2, int d1, T *data) {
-  t213_throw_on(t213_rotate(f.kind, (const int64_t *)f.p, f.np, data, d3, d2, d1, (int)sizeof(T), 0),
+  t213_throw_on(t213_rotate(f.kind, f.p, f.np, data, d3, d2, d1, (int)sizeof(T), 0),
                 "inplace::detail::rotate");
   t213_throw_on(t213_sync_default_stream(), "inplace::detail::rotate");
 }
@@ -100,7 +102,7 @@ void rotate(F f, int d3, int d2, int d1, T *data) {
 /* include/shuffle.h:5-6 */
 template <typename T, typename F>
 void shuffle_fn(T *data, int d3, int d2, int d1, F s) {
-  t213_throw_on(t213_row_shuffle(s.kind, (const int64_t *)s.p, s.np, data, d3, d2, d1, (int)sizeof(T), 0),
+  t213_throw_on(t213_row_shuffle(s.kind, s.p, s.np, data, d3, d2, d1, (int)sizeof(T), 0),
                 "inplace::detail::shuffle_fn");
   t213_throw_on(t213_sync_default_stream(), "inplace::detail::shuffle_fn");
 }
@@ -108,7 +110,7 @@ void shuffle_fn(T *data, int d3, int d2, int d1, F s) {
 /* include/col_shuffle.h:8-9 */
 template <typename F, typename T>
 void col_shuffle_fn(F fn, int d3, int d2, int d1, T *data) {
-  t213_throw_on(t213_col_shuffle(fn.kind, (const int64_t *)fn.p, fn.np, data, d3, d2, d1, (int)sizeof(T), 0),
+  t213_throw_on(t213_col_shuffle(fn.kind, fn.p, fn.np, data, d3, d2, d1, (int)sizeof(T), 0),
                 "inplace::detail::col_shuffle_fn");
   t213_throw_on(t213_sync_default_stream(), "inplace::detail::col_shuffle_fn");
 }
@@ -116,7 +118,7 @@ void col_shuffle_fn(F fn, int d3, int d2, int d1, T *data) {
 /* include/permute.h:6-7 */
 template <typename T, typename F>
 void scatter_permute(F f, int d3, int d2, int d1, T *data) {
-  t213_throw_on(t213_scatter_permute(f.kind, (const int64_t *)f.p, f.np, data, d3, d2, d1, (int)sizeof(T), 0),
+  t213_throw_on(t213_scatter_permute(f.kind, f.p, f.np, data, d3, d2, d1, (int)sizeof(T), 0),
                 "inplace::detail::scatter_permute");
   t213_throw_on(t213_sync_default_stream(), "inplace::detail::scatter_permute");
 }

@@ -208,6 +208,16 @@ int t213_batch_execute(t213_batch batch, t213_stream_t stream);
  * bounded wait ran out).  Synchronises the stream. */
 int t213_batch_status(t213_batch batch, t213_stream_t stream);
 int t213_batch_describe(t213_batch batch, char *buf, size_t buflen);
+/* Test hook of the batch's failure path.  Limits every dependency wait of the
+ * persistent kernel to wait_ns nanoseconds and makes pass stall_pass (-1: the
+ * first pass that has a predecessor) wait for one item more than its
+ * predecessor has, so that wait can only end by running out.  The next
+ * t213_batch_execute runs with these settings (a captured graph is dropped),
+ * its CTAs leave on the timeout, the launch completes, and t213_batch_status
+ * then returns T213_ERR_TIMEOUT once.  The batch's tensors are left partly
+ * transposed.  Replaces no reference interface: the reference's grid-wide
+ * waits (src/memory_ops.cu:18-33, src/skinny.cu:31-60) are unbounded. */
+int t213_batch_debug_stall(t213_batch batch, int64_t wait_ns, int32_t stall_pass);
 int t213_batch_destroy(t213_batch batch);
 /* Autotunes every shape class present in the list (timing the applicable
  * plan families on scratch memory of the class's largest tensor) so that

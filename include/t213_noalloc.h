@@ -35,8 +35,14 @@ extern "C" {
  * The scratch is shared by every call on a device: calls that overlap in time
  * (on different streams, or from different host threads) race on it and
  * corrupt each other's results, so serialise them.
- * The first call on each device does the set-up (it looks up the scratch
- * address and sets kernel attributes): make it before any concurrent use.
+ * The first call on each device does the set-up: it looks up the scratch's
+ * device address and the device's SM count.  Under CUDA's default lazy module
+ * loading this is also when the driver loads the library's module holding
+ * the array onto the device, reserving its 32 MiB there.  So make the first
+ * call on a device before your own allocator fills the device's memory; an
+ * empty call (d1, d2 or d3 zero, valid parameters otherwise) does only the
+ * set-up and serves as the warm-up.  Set-up itself is thread-safe; it is the
+ * scratch that concurrent calls must not share.
  * Nothing has to start at zero: each call writes every scratch byte it reads.
  * Asynchronous on `stream` like t213_row_shuffle. */
 int t213_row_shuffle_noalloc(int32_t fn_kind, const int64_t *fn_params, int32_t n_params, void *data,

@@ -53,12 +53,14 @@ _lib = None
 _ref = None
 
 
-def build() -> None:
-    """Compiles liboracle213.so (and, when the reference tree is present, the
-    reference's CPU and GPU builds under _ref/)."""
+def build(reference: str | None = None) -> None:
+    """Compiles liboracle213.so and, when the reference's source tree is given
+    (argument, or the environment's T213_REFERENCE) and present, the
+    reference's CPU and GPU builds under _ref/."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
-    if os.path.isdir(os.environ.get("T213_REFERENCE", "/root/reference")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    ref = reference or os.environ.get("T213_REFERENCE")
+    if ref and os.path.isdir(os.path.join(ref, "src")):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True)
 
 
 def lib() -> ctypes.CDLL:

@@ -8,15 +8,26 @@
 #include <cuda_runtime.h>
 #include "transpose.h"
 
-extern "C" int ref_inplace_transpose(void *data, int d1, int d2, int d3, int type_size) {
-  if (type_size == 4)
-    inplace::transpose(static_cast<int *>(data), d1, d2, d3);
-  else if (type_size == 8)
-    inplace::transpose(static_cast<long long *>(data), d1, d2, d3);
-  else
-    return -1;
+// type codes of ref_inplace_transpose_typed: the four instantiations of the
+// reference's dispatcher (src/transpose.cu:126-129)
+enum { REF_INT32 = 0, REF_FLOAT = 1, REF_INT64 = 2, REF_DOUBLE = 3 };
+
+extern "C" int ref_inplace_transpose_typed(void *data, int d1, int d2, int d3, int code) {
+  switch (code) {
+    case REF_INT32: inplace::transpose(static_cast<int *>(data), d1, d2, d3); break;
+    case REF_FLOAT: inplace::transpose(static_cast<float *>(data), d1, d2, d3); break;
+    case REF_INT64: inplace::transpose(static_cast<long long *>(data), d1, d2, d3); break;
+    case REF_DOUBLE: inplace::transpose(static_cast<double *>(data), d1, d2, d3); break;
+    default: return -1;
+  }
   cudaError_t e = cudaDeviceSynchronize();
   return e == cudaSuccess ? 0 : (int)e;
+}
+
+extern "C" int ref_inplace_transpose(void *data, int d1, int d2, int d3, int type_size) {
+  if (type_size == 4) return ref_inplace_transpose_typed(data, d1, d2, d3, REF_INT32);
+  if (type_size == 8) return ref_inplace_transpose_typed(data, d1, d2, d3, REF_INT64);
+  return -1;
 }
 
 extern "C" void *ref_alloc_managed(size_t bytes) {

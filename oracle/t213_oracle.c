@@ -29,9 +29,9 @@
  * used only to explain divergences of the reference's GPU build:
  *   T213O_REF_POSTOP_BUG  c2r::col_op's fused branch passes d2/c where the math
  *                         needs c (src/transpose.cu:22).
- *   T213O_REF_REG8_BUG    the 8-byte register row shuffles launch without a
- *                         slice offset, so only slice 0 is shuffled, and the
- *                         R=57 variant covers only 57*512 columns
+ *   T213O_REF_REG8_BUG    the 8-byte register row shuffles (C2R and R2C) launch
+ *                         without a slice offset, so only slice 0 is shuffled,
+ *                         and the R=57 variant covers only 57*512 columns
  *                         (src/shuffle.cu:40-49, include/register_ops.h:66-80).
  */
 #include <stdint.h>
@@ -424,6 +424,25 @@ static void r2c_consts(i64 m, i64 n, i64 *c, i64 *q) {
     *q = t;
 }
 
+/* The reference's row-shuffle dispatch (src/shuffle.cu:12-64) for both
+ * shufflers.  Every variant computes the same gather, except that with
+ * T213O_REF_REG8_BUG the 8-byte register variants (rows over 48 KB and under
+ * 29696 columns) are launched without a slice offset, so only slice 0 is
+ * shuffled, and R = 57 registers of 512 threads cover 57 * 512 columns
+ * (src/shuffle.cu:40-49, include/register_ops.h:66-80). */
+static int ref_row_shuffle(const fn_t *f, char *data, i64 d3, i64 m, i64 n, i64 eb, int flags) {
+  i64 slices = d3, maxc = n;
+  if ((flags & T213O_REF_REG8_BUG) && eb == 8) {
+    int compress = 2 * n * eb <= T213O_SMEM_PER_BLOCK / 32;
+    int smem = n * eb <= T213O_SMEM_PER_BLOCK;
+    if (!compress && !smem && n < 29696) {
+      slices = 1;
+      maxc = (n < 6918) ? 18 * 512 : 57 * 512;
+    }
+  }
+  return row_shuffle_impl(f, data, d3, m, n, eb, slices, maxc);
+}
+
 /* C2R: the slice is m = d2 rows x n = d1 columns (src/transpose.cu:18-47).
  * The column op is the fused column shuffle when a 32-column strip of the
  * slice fits the reference's 48 KB shared-memory limit, else a post-rotation
@@ -439,17 +458,7 @@ int t213o_c2r(void *data, i64 d1, i64 d2, i64 d3, i64 eb, int flags) {
   }
   {
     fn_t f = mkfn(T213_FN_C2R_SHUFFLE, (i64[4]){m, n, c, k});
-    i64 slices = d3, maxc = n;
-    if ((flags & T213O_REF_REG8_BUG) && eb == 8) {
-      /* src/shuffle.cu:25-49: register variants for 8-byte rows over 48 KB */
-      int compress = 2 * n * eb <= T213O_SMEM_PER_BLOCK / 32;
-      int smem = n * eb <= T213O_SMEM_PER_BLOCK;
-      if (!compress && !smem && n < 29696) {
-        slices = 1;
-        maxc = (n < 6918) ? 18 * 512 : 57 * 512;
-      }
-    }
-    if ((rc = row_shuffle_impl(&f, (char *)data, d3, m, n, eb, slices, maxc))) return rc;
+    if ((rc = ref_row_shuffle(&f, (char *)data, d3, m, n, eb, flags))) return rc;
   }
   if (T213O_SMEM_PER_BLOCK / (eb * m) >= 32) {
     i64 third = (flags & T213O_REF_POSTOP_BUG) ? m / c : c;
@@ -469,7 +478,6 @@ int t213o_c2r(void *data, i64 d1, i64 d2, i64 d3, i64 eb, int flags) {
  * shape; the input is the n x m matrix. */
 int t213o_r2c(void *data, i64 d1, i64 d2, i64 d3, i64 eb, int flags) {
   i64 m = d2, n = d1, c, q;
-  (void)flags;
   if (m <= 0 || n <= 0 || d3 <= 0) return 0;
   r2c_consts(m, n, &c, &q);
   int rc;
@@ -483,8 +491,8 @@ int t213o_r2c(void *data, i64 d1, i64 d2, i64 d3, i64 eb, int flags) {
     if ((rc = t213o_rotate(T213_FN_R2C_PREROTATOR, r, data, d3, m, n, eb))) return rc;
   }
   {
-    i64 p[4] = {m, n, c, q};
-    if ((rc = t213o_row_shuffle(T213_FN_R2C_SHUFFLE, p, data, d3, m, n, eb))) return rc;
+    fn_t f = mkfn(T213_FN_R2C_SHUFFLE, (i64[4]){m, n, c, q});
+    if ((rc = ref_row_shuffle(&f, (char *)data, d3, m, n, eb, flags))) return rc;
   }
   if (c > 1) {
     i64 p[4] = {n / c, m, 0, 0};
