@@ -237,6 +237,18 @@ def run_ours(args):
     del oop, xv, ov
     torch.cuda.empty_cache()
 
+    # the same tensor through the reference's own decomposition (C2R forced)
+    c2r_plan = t213.describe(D1, D2, D3, EB, "c2r")
+    for _ in range(args.warmup):
+        t213.transpose_with_plan(x, D1, D2, D3, "c2r")
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(args.steps):
+        t213.transpose_with_plan(x, D1, D2, D3, "c2r")
+    b.record(stream)
+    b.synchronize()
+    ms_c2r = max_over_ranks(dist, a.elapsed_time(b)) / args.steps
+
     # secondary tensor: fp64 (7919, 6151, 2)
     nb2 = D1B * D2B * D3B * EBB
     y = torch.empty(D1B * D2B * D3B, dtype=torch.float64, device=dev).uniform_(-1, 1, generator=gen)
@@ -249,6 +261,14 @@ def run_ours(args):
     b.record(stream)
     b.synchronize()
     ms_b = max_over_ranks(dist, a.elapsed_time(b))
+    t213.pass_timing.reset()
+    t213.pass_timing.enable(True)
+    for _ in range(args.steps):
+        t213.transpose(y, D1B, D2B, D3B)
+    torch.cuda.synchronize()
+    per_b = {p: t213.pass_timing.read(p) for p in PASSES}
+    t213.pass_timing.enable(False)
+    per_b = {k: v for k, v in per_b.items() if v[1] > 0}
     del y
     torch.cuda.empty_cache()
 
@@ -267,10 +287,11 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample()
-    batched = serving = None
+    batched = serving = configs = None
     if world == 1 and not args.quick:
         del x
         torch.cuda.empty_cache()
+        configs = configs_section(t213, torch, args.steps, args.warmup)
         batched = batched_section(t213, torch, stream)
         serving = serving_section(t213, torch)
 
@@ -291,9 +312,16 @@ def run_ours(args):
                          "peak_source": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": traffic,
                          "algorithmic_bytes_per_launch": 2 * nbytes},
+            "forced_c2r": {"what": "the headline tensor through the reference's C2R decomposition (forced plan)",
+                           "plan": c2r_plan, "ms": round(ms_c2r, 4),
+                           "value": round(world * 2 * nbytes / (ms_c2r * 1e-3) / 1e9, 1), "unit": UNIT},
             "secondary": {"workload": f"fp64 (7919,6151,2) {nb2 / 1e6:.1f} MB",
                           "plan": t213.describe(D1B, D2B, D3B, EBB),
-                          "value": round(world * 2 * nb2 * args.steps / (ms_b * 1e-3) / 1e9, 1), "unit": UNIT},
+                          "value": round(world * 2 * nb2 * args.steps / (ms_b * 1e-3) / 1e9, 1), "unit": UNIT,
+                          "roofline": {k: {"ms_per_launch": round(v[0] / v[1], 4),
+                                           "achieved": round(2 * nb2 / (v[0] / v[1] * 1e-3) / 1e9, 1),
+                                           "frac": round(2 * nb2 / (v[0] / v[1] * 1e-3) / 1e9 / peak, 4)}
+                                       for k, v in per_b.items()}},
             "out_of_place_torch": {"what": "torch x.view(d3,d2,d1).transpose(1,2) copied into a second buffer "
                                            "(out of place: one sweep, 2x memory)",
                                    "ms": round(ms_oop, 4), "GBps": round(2 * nbytes / (ms_oop * 1e-3) / 1e9, 1),
@@ -306,6 +334,8 @@ def run_ours(args):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if configs:
+            line["configs"] = configs
         if batched:
             line["batched"] = batched
         if serving:
@@ -313,6 +343,67 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+
+
+# ------------------------------------------------------- other configs -----
+CONFIGS = [  # name, d1, d2, d3, element bytes
+    ("fp32 (512,384,16)", 512, 384, 16, 4),
+    ("fp32 (32,2^24,1)", 32, 1 << 24, 1, 4),
+    ("fp32 (2^24,48,1)", 1 << 24, 48, 1, 4),
+    ("int32 (3,2^22,8)", 3, 1 << 22, 8, 4),
+    ("16B (1024,1024,1)", 1024, 1024, 1, 16),
+]
+
+
+def configs_section(t213, torch, steps, warmup):
+    """The workload's other single-tensor configurations, device-resident,
+    random bit patterns: the plain call timed with CUDA events over `steps`
+    calls, and for tensors under 64 MB also one call captured in a CUDA graph
+    and replayed (launch latency off the critical path)."""
+    out = []
+    for name, d1, d2, d3, eb in CONFIGS:
+        n = d1 * d2 * d3 * eb
+        x = torch.empty(n, dtype=torch.uint8, device="cuda")
+        x.random_(0, 256, generator=torch.Generator(device="cuda").manual_seed(3))
+
+        def call():
+            t213.transpose(x, d1, d2, d3, elem_bytes=eb)
+
+        def timed(fn):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            for _ in range(warmup):
+                fn()
+            torch.cuda.synchronize()
+            a.record(torch.cuda.current_stream())
+            for _ in range(steps):
+                fn()
+            b.record(torch.cuda.current_stream())
+            b.synchronize()
+            return a.elapsed_time(b) / steps
+
+        ms = timed(call)
+        e = {"config": name, "plan": t213.describe(d1, d2, d3, eb), "MB": round(n / 1e6, 1), "ms": round(ms, 4),
+             "GBps": round(2 * n / (ms * 1e-3) / 1e9, 1)}
+        if n < (64 << 20):
+            try:
+                side = torch.cuda.Stream()
+                with torch.cuda.stream(side):
+                    call()  # plan and workspace for this stream, outside the capture
+                torch.cuda.synchronize()
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g, stream=side):
+                    call()
+                msg = timed(g.replay)
+                e["graph_ms"] = round(msg, 4)
+                e["graph_GBps"] = round(2 * n / (msg * 1e-3) / 1e9, 1)
+                del g
+            except Exception as ex:  # capture is optional: report why it did not happen
+                e["graph_error"] = str(ex)[:200]
+        out.append(e)
+        del x
+        torch.cuda.empty_cache()
+    return out
 
 
 # ------------------------------------------------------ batched / serving ----
