@@ -51,7 +51,9 @@ class ServeStats(ctypes.Structure):
     _fields_ = [("completed", ctypes.c_int64), ("rejected", ctypes.c_int64), ("bytes_done", ctypes.c_int64),
                 ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
                 ("max_ms", ctypes.c_double), ("wall_s", ctypes.c_double), ("peak_resident_bytes", ctypes.c_int64),
-                ("max_inflight", ctypes.c_int64)]
+                ("max_inflight", ctypes.c_int64), ("cold", ctypes.c_int64), ("p50_cold_ms", ctypes.c_double),
+                ("p99_cold_ms", ctypes.c_double), ("p50_warm_ms", ctypes.c_double), ("p99_warm_ms", ctypes.c_double),
+                ("group_launches", ctypes.c_int64), ("grouped_requests", ctypes.c_int64)]
 
 
 _lib = None
@@ -98,6 +100,9 @@ _SIGS = {
     "t213_server_create": ([_i64, _i32, _i32, ctypes.POINTER(_vp)], ctypes.c_int),
     "t213_server_run": ([_vp, ctypes.POINTER(Request), _i32, ctypes.POINTER(ServeStats),
                          ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+    "t213_server_run_capture": ([_vp, ctypes.POINTER(Request), _i32, ctypes.POINTER(ServeStats),
+                                 ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double),
+                                 ctypes.POINTER(_vp)], ctypes.c_int),
     "t213_server_expected_checksum": ([_vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
     "t213_server_run_alone": ([_vp, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_uint64)], ctypes.c_int),
     "t213_server_destroy": ([_vp], ctypes.c_int),

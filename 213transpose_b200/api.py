@@ -289,14 +289,30 @@ class Server:
                                   float(r.get("t", r.get("arrival_s", 0.0))), int(r.get("seed", i + 1)))
         return arr
 
-    def run(self, reqs):
-        """Replays the schedule; returns (stats dict, checksums, latencies_ms)."""
+    def run(self, reqs, capture=None):
+        """Replays the schedule; returns (stats dict, checksums, latencies_ms).
+        `capture` maps request indices to writable host buffers (numpy arrays
+        or pinned torch tensors of the request's byte size) that receive the
+        transposed tensor."""
         n = len(reqs)
         arr = self._requests(reqs)
         st = _lib.ServeStats()
         sums = (ctypes.c_uint64 * max(1, n))()
         lat = (ctypes.c_double * max(1, n))()
-        check(lib().t213_server_run(self._h, arr, n, ctypes.byref(st), sums, lat))
+        outs = None
+        if capture:
+            outs = (ctypes.c_void_p * max(1, n))()
+            for i, buf in capture.items():
+                r = reqs[i]
+                need = int(r["d1"]) * int(r["d2"]) * int(r["d3"]) * int(r["elem_bytes"])
+                if hasattr(buf, "data_ptr"):
+                    size, ptr = buf.numel() * buf.element_size(), buf.data_ptr()
+                else:
+                    size, ptr = buf.nbytes, buf.ctypes.data
+                if size < need:
+                    raise ValueError(f"capture buffer of request {i} holds {size} bytes, needs {need}")
+                outs[i] = ptr
+        check(lib().t213_server_run_capture(self._h, arr, n, ctypes.byref(st), sums, lat, outs))
         stats = {f: getattr(st, f) for f, _ in _lib.ServeStats._fields_}
         return stats, list(sums)[:n], list(lat)[:n]
 

@@ -49,6 +49,13 @@ struct t213_batch_st {
 
 namespace {
 
+struct BatchTables {
+  std::vector<BPass> passes;
+  std::vector<BItem> items;
+  std::vector<size_t> carry_off;  // per cycle pass with carries (its CARRY and SEG passes share it)
+  size_t carry_bytes = 0;
+};
+
 // Target bytes read per queue item: small enough that one tensor's pass
 // spreads over many SMs (the batch's critical path is the chain of passes of
 // its slowest tensor), large enough that the queue overhead stays small.
@@ -171,79 +178,25 @@ bool plan_fits_batch(const Plan &p) {
   return true;
 }
 
-}  // namespace
-
-extern "C" {
-
-int t213_transpose_looped(const t213_tensor_desc *tensors, int32_t count, t213_stream_t stream) {
-  if (count < 0 || (count > 0 && !tensors)) return T213_ERR_INVALID_ARGUMENT;
-  for (int32_t i = 0; i < count; i++) {
-    const t213_tensor_desc &d = tensors[i];
-    int rc = d.plan_kind == T213_PLAN_AUTO
-                 ? t213_transpose(d.data, d.d1, d.d2, d.d3, d.elem_bytes, stream)
-                 : t213_transpose_with_plan(d.data, d.d1, d.d2, d.d3, d.elem_bytes, d.plan_kind, 0, stream);
-    if (rc) return rc;
-  }
-  return T213_OK;
-}
-
-int t213_batch_create(const t213_tensor_desc *tensors, int32_t count, t213_batch *out) {
-  if (!out || count < 0 || (count > 0 && !tensors)) {
-    set_error("t213_batch_create: bad arguments");
-    return T213_ERR_INVALID_ARGUMENT;
-  }
-  *out = nullptr;
-  auto *B = new t213_batch_st();
-  B->dev = dev_info().id;
-  B->tensors.assign(tensors, tensors + count);
-  int rc = T213_OK;
-  auto fail = [&](int code) {
-    t213_batch_destroy(B);
-    return code;
-  };
-
-  // ---- plans ---------------------------------------------------------------
-  std::vector<int> per_tensor_first_pass(count, -1), per_tensor_npass(count, 0);
-  std::vector<std::vector<int>> tensor_passes(count);
-  for (int32_t i = 0; i < count; i++) {
-    const t213_tensor_desc &d = tensors[i];
-    if (d.d1 < 0 || d.d2 < 0 || d.d3 < 0 || (d.elem_bytes != 1 && d.elem_bytes != 2 && d.elem_bytes != 4 &&
-                                              d.elem_bytes != 8 && d.elem_bytes != 16)) {
-      set_error("t213_batch_create: bad tensor descriptor");
-      return fail(T213_ERR_INVALID_ARGUMENT);
-    }
-    if (d.d1 * d.d2 * d.d3 > 0 && !d.data) {
-      set_error("t213_batch_create: NULL data");
-      return fail(T213_ERR_INVALID_ARGUMENT);
-    }
-    B->total_bytes += d.d1 * d.d2 * d.d3 * d.elem_bytes;
-    std::shared_ptr<Plan> P;
-    if (d.d1 * d.d2 * d.d3 > 0) {
-      P = get_plan(d.d1, d.d2, d.d3, d.elem_bytes, d.plan_kind, 0, &rc);
-      if (!P) return fail(rc);
-      if (!plan_fits_batch(*P) && d.plan_kind == T213_PLAN_AUTO) {
-        // another family that fits the persistent kernel's shared memory
-        for (int k : {T213_PLAN_BLOCKS, T213_PLAN_BANDS, T213_PLAN_BANDS_T, T213_PLAN_C2R, T213_PLAN_R2C}) {
-          int rc2 = T213_OK;
-          auto Q = get_plan(d.d1, d.d2, d.d3, d.elem_bytes, k, 0, &rc2);
-          if (Q && plan_fits_batch(*Q)) {
-            P = Q;
-            break;
-          }
-        }
-      }
-      if (!plan_fits_batch(*P) || d.d1 * d.d2 * d.d3 * d.elem_bytes > direct_threshold()) B->spill.push_back(i);
-    }
-    B->plans.push_back(P);
-  }
-
+// Flattens the plans of the tensors (plans[i] null or skip[i] set: left out)
+// into the persistent kernel's pass table and its level-ordered item queue,
+// and lays out the carry pool the cycle passes need (bind_carry points them
+// at it).
+int build_batch_tables(const t213_tensor_desc *tensors, int32_t count, const std::vector<std::shared_ptr<Plan>> &plans,
+                       const std::vector<char> &skip, BatchTables &T) {
+  T.passes.clear();
+  T.items.clear();
+  T.carry_off.clear();
+  T.carry_bytes = 0;
   // ---- passes ------------------------------------------------------------------
   size_t carry_total = 0;
-  std::vector<size_t> carry_off;
+  std::vector<size_t> &carry_off = T.carry_off;
+  std::vector<std::vector<int>> tensor_passes(count);
+  int rc = T213_OK;
   for (int32_t i = 0; i < count; i++) {
     const t213_tensor_desc &d = tensors[i];
-    const std::shared_ptr<Plan> &P = B->plans[i];
-    if (!P || std::find(B->spill.begin(), B->spill.end(), i) != B->spill.end()) continue;
+    const std::shared_ptr<Plan> &P = plans[i];
+    if (!P || skip[i]) continue;
     const int eb = d.elem_bytes;
     char *data = (char *)d.data;
     const int64_t slice_bytes = d.d1 * d.d2 * eb;
@@ -311,7 +264,7 @@ int t213_batch_create(const t213_tensor_desc *tensors, int32_t count, t213_batch
           const CycleTable &ct = *q.table;
           if ((rc = const_cast<CycleTable &>(ct).ensure_uploaded(nullptr)) ||
               (rc = const_cast<CycleTable &>(ct).wait_uploaded()))
-            return fail(rc);
+            return rc;
           bp.seg_bytes = q.seg_bytes;
           bp.seg_aw = seg_access_width(data, q.seg_bytes, slice_bytes);
           bp.chunks = (const Chunk *)ct.d_chunks;
@@ -327,8 +280,8 @@ int t213_batch_create(const t213_tensor_desc *tensors, int32_t count, t213_batch
             BPass cp = bp;
             cp.kind = BK_CARRY;
             cp.n_units = ct.n_carry * d.d3;
-            B->h_passes.push_back(cp);
-            tensor_passes[i].push_back((int)B->h_passes.size() - 1);
+            T.passes.push_back(cp);
+            tensor_passes[i].push_back((int)T.passes.size() - 1);
             carry_off.push_back(carry_total);
             carry_total += (size_t)(ct.n_carry * d.d3 * q.seg_bytes + 255) / 256 * 256;
           }
@@ -342,30 +295,18 @@ int t213_batch_create(const t213_tensor_desc *tensors, int32_t count, t213_batch
         }
       }
       if (bp.n_units == 0) continue;
-      B->h_passes.push_back(bp);
-      tensor_passes[i].push_back((int)B->h_passes.size() - 1);
+      T.passes.push_back(bp);
+      tensor_passes[i].push_back((int)T.passes.size() - 1);
     }
   }
-  // carry pool
-  if (carry_total > 0) {
-    cudaError_t e = cudaMalloc(&B->d_carry, carry_total);
-    if (e != cudaSuccess) return fail(cuda_status(e, "batch carry pool"));
-    B->carry_bytes = carry_total;
-    size_t ci = 0;
-    for (BPass &bp : B->h_passes)
-      if ((bp.kind == BK_CARRY || bp.kind == BK_SEG) && bp.n_carry > 0) bp.carry_buf = B->d_carry + carry_off[ci++];
-  }
-
-  // ---- items, level by level -------------------------------------------------------
-  B->n_ctrs = (int)B->h_passes.size();
-  std::vector<int64_t> items_of_pass(B->h_passes.size(), 0);
+  std::vector<int64_t> items_of_pass(T.passes.size(), 0);
   size_t max_levels = 0;
   for (auto &tp : tensor_passes) max_levels = std::max(max_levels, tp.size());
   for (size_t lvl = 0; lvl < max_levels; lvl++) {
     for (int32_t i = 0; i < count; i++) {
       if (lvl >= tensor_passes[i].size()) continue;
       const int pi = tensor_passes[i][lvl];
-      BPass &bp = B->h_passes[pi];
+      BPass &bp = T.passes[pi];
       bp.done_ctr = pi;
       if (lvl > 0) {
         const int prev = tensor_passes[i][lvl - 1];
@@ -399,11 +340,216 @@ int t213_batch_create(const t213_tensor_desc *tensors, int32_t count, t213_batch
           break;
       }
       for (int64_t u = 0; u < bp.n_units; u += upi) {
-        B->h_items.push_back(BItem{pi, 0, u, std::min(bp.n_units, u + upi)});
+        T.items.push_back(BItem{pi, 0, u, std::min(bp.n_units, u + upi)});
         items_of_pass[pi]++;
       }
     }
   }
+  T.carry_bytes = carry_total;
+  return T213_OK;
+}
+
+void bind_carry(std::vector<BPass> &passes, const std::vector<size_t> &carry_off, char *pool) {
+  size_t ci = 0;
+  for (BPass &bp : passes)
+    if ((bp.kind == BK_CARRY || bp.kind == BK_SEG) && bp.n_carry > 0) bp.carry_buf = pool + carry_off[ci++];
+}
+
+}  // namespace
+
+namespace t213 {
+
+std::shared_ptr<Plan> group_plan(int64_t d1, int64_t d2, int64_t d3, int eb, int *status) {
+  std::shared_ptr<Plan> P = get_plan(d1, d2, d3, eb, T213_PLAN_AUTO, 0, status);
+  if (!P) return nullptr;
+  if (plan_fits_batch(*P)) return P;
+  // another family that fits the persistent kernel's shared memory
+  for (int k : {T213_PLAN_BLOCKS, T213_PLAN_BANDS, T213_PLAN_BANDS_T, T213_PLAN_C2R, T213_PLAN_R2C}) {
+    int rc2 = T213_OK;
+    auto Q = get_plan(d1, d2, d3, eb, k, 0, &rc2);
+    if (Q && plan_fits_batch(*Q)) return Q;
+  }
+  return nullptr;
+}
+
+struct GroupExec {
+  int dev = 0;
+  int64_t cap_passes = 0, cap_items = 0;
+  size_t cap_carry = 0;
+  BPass *d_passes = nullptr, *h_passes = nullptr;  // device table and its pinned staging
+  BItem *d_items = nullptr, *h_items = nullptr;
+  unsigned long long *d_ctrs = nullptr;  // one per pass, then the queue head
+  int *d_status = nullptr, *h_status = nullptr;
+  char *d_carry = nullptr;
+  int grid = 0;
+  cudaEvent_t done = nullptr;
+  bool launched = false;
+};
+
+GroupExec *group_exec_create(int64_t max_passes, int64_t max_items, size_t carry_bytes, int *status) {
+  *status = T213_OK;
+  auto *g = new GroupExec();
+  g->dev = dev_info().id;
+  g->cap_passes = max_passes;
+  g->cap_items = max_items;
+  g->cap_carry = carry_bytes;
+  cudaError_t e = cudaSuccess;
+  if (!e) e = cudaMalloc(&g->d_passes, max_passes * sizeof(BPass));
+  if (!e) e = cudaMallocHost(&g->h_passes, max_passes * sizeof(BPass));
+  if (!e) e = cudaMalloc(&g->d_items, max_items * sizeof(BItem));
+  if (!e) e = cudaMallocHost(&g->h_items, max_items * sizeof(BItem));
+  if (!e) e = cudaMalloc(&g->d_ctrs, (max_passes + 1) * sizeof(unsigned long long));
+  if (!e) e = cudaMalloc(&g->d_status, 256);
+  if (!e) e = cudaMallocHost(&g->h_status, sizeof(int));
+  if (!e && carry_bytes) e = cudaMalloc(&g->d_carry, carry_bytes);
+  if (!e) e = cudaMemset(g->d_status, 0, 256);
+  if (!e) e = cudaEventCreateWithFlags(&g->done, cudaEventDisableTiming);
+  if (!e) e = cudaFuncSetAttribute(k_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(kBatchSmem + kBatchBarBytes));
+  if (!e) e = cudaDeviceSynchronize();  // the memset ran on the legacy stream
+  if (e) {
+    *status = cuda_status(e, "group executor");
+    group_exec_destroy(g);
+    return nullptr;
+  }
+  *g->h_status = 0;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch, kBatchThreads,
+                                                    (size_t)(kBatchSmem + kBatchBarBytes)) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  g->grid = per_sm * dev_info().sms;
+  return g;
+}
+
+void group_exec_destroy(GroupExec *g) {
+  if (!g) return;
+  if (g->done) {
+    cudaEventSynchronize(g->done);
+    cudaEventDestroy(g->done);
+  }
+  cudaFree(g->d_passes);
+  cudaFreeHost(g->h_passes);
+  cudaFree(g->d_items);
+  cudaFreeHost(g->h_items);
+  cudaFree(g->d_ctrs);
+  cudaFree(g->d_status);
+  cudaFreeHost(g->h_status);
+  cudaFree(g->d_carry);
+  delete g;
+}
+
+bool group_exec_idle(GroupExec *g) { return !g->launched || cudaEventQuery(g->done) == cudaSuccess; }
+
+int group_exec_status(GroupExec *g) { return *g->h_status; }
+
+int group_exec_run(GroupExec *g, const t213_tensor_desc *tensors, int32_t count, cudaStream_t st) {
+  std::vector<std::shared_ptr<Plan>> plans(count);
+  for (int32_t i = 0; i < count; i++) {
+    const t213_tensor_desc &d = tensors[i];
+    if (d.d1 * d.d2 * d.d3 == 0) continue;
+    int rc = T213_OK;
+    plans[i] = group_plan(d.d1, d.d2, d.d3, d.elem_bytes, &rc);
+    if (!plans[i]) return T213_ERR_UNSUPPORTED;
+  }
+  BatchTables T;
+  int rc = build_batch_tables(tensors, count, plans, std::vector<char>(count, 0), T);
+  if (rc) return rc;
+  if ((int64_t)T.passes.size() > g->cap_passes || (int64_t)T.items.size() > g->cap_items ||
+      T.carry_bytes > g->cap_carry)
+    return T213_ERR_UNSUPPORTED;
+  if (T.items.empty()) return T213_OK;
+  bind_carry(T.passes, T.carry_off, g->d_carry);
+  // the staging is free: the previous launch, and with it its table copies, finished
+  memcpy(g->h_passes, T.passes.data(), T.passes.size() * sizeof(BPass));
+  memcpy(g->h_items, T.items.data(), T.items.size() * sizeof(BItem));
+  cudaError_t e = cudaMemcpyAsync(g->d_passes, g->h_passes, T.passes.size() * sizeof(BPass),
+                                  cudaMemcpyHostToDevice, st);
+  if (!e) e = cudaMemcpyAsync(g->d_items, g->h_items, T.items.size() * sizeof(BItem), cudaMemcpyHostToDevice, st);
+  if (!e) e = cudaMemsetAsync(g->d_ctrs, 0, (T.passes.size() + 1) * sizeof(unsigned long long), st);
+  if (e) return cuda_status(e, "group tables");
+  k_batch<<<g->grid, kBatchThreads, (size_t)(kBatchSmem + kBatchBarBytes), st>>>(
+      g->d_passes, g->d_items, (int64_t)T.items.size(), g->d_ctrs, g->d_ctrs + T.passes.size(), g->d_status,
+      kWaitNs);
+  e = cudaGetLastError();
+  if (!e) e = cudaMemcpyAsync(g->h_status, g->d_status, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (!e) e = cudaMemsetAsync(g->d_status, 0, sizeof(int), st);
+  if (!e) e = cudaEventRecord(g->done, st);
+  if (e) return cuda_status(e, "group launch");
+  g->launched = true;
+  return T213_OK;
+}
+
+}  // namespace t213
+
+extern "C" {
+
+int t213_transpose_looped(const t213_tensor_desc *tensors, int32_t count, t213_stream_t stream) {
+  if (count < 0 || (count > 0 && !tensors)) return T213_ERR_INVALID_ARGUMENT;
+  for (int32_t i = 0; i < count; i++) {
+    const t213_tensor_desc &d = tensors[i];
+    int rc = d.plan_kind == T213_PLAN_AUTO
+                 ? t213_transpose(d.data, d.d1, d.d2, d.d3, d.elem_bytes, stream)
+                 : t213_transpose_with_plan(d.data, d.d1, d.d2, d.d3, d.elem_bytes, d.plan_kind, 0, stream);
+    if (rc) return rc;
+  }
+  return T213_OK;
+}
+
+int t213_batch_create(const t213_tensor_desc *tensors, int32_t count, t213_batch *out) {
+  if (!out || count < 0 || (count > 0 && !tensors)) {
+    set_error("t213_batch_create: bad arguments");
+    return T213_ERR_INVALID_ARGUMENT;
+  }
+  *out = nullptr;
+  auto *B = new t213_batch_st();
+  B->dev = dev_info().id;
+  B->tensors.assign(tensors, tensors + count);
+  int rc = T213_OK;
+  auto fail = [&](int code) {
+    t213_batch_destroy(B);
+    return code;
+  };
+
+  // ---- plans ---------------------------------------------------------------
+  for (int32_t i = 0; i < count; i++) {
+    const t213_tensor_desc &d = tensors[i];
+    if (d.d1 < 0 || d.d2 < 0 || d.d3 < 0 || (d.elem_bytes != 1 && d.elem_bytes != 2 && d.elem_bytes != 4 &&
+                                              d.elem_bytes != 8 && d.elem_bytes != 16)) {
+      set_error("t213_batch_create: bad tensor descriptor");
+      return fail(T213_ERR_INVALID_ARGUMENT);
+    }
+    if (d.d1 * d.d2 * d.d3 > 0 && !d.data) {
+      set_error("t213_batch_create: NULL data");
+      return fail(T213_ERR_INVALID_ARGUMENT);
+    }
+    B->total_bytes += d.d1 * d.d2 * d.d3 * d.elem_bytes;
+    std::shared_ptr<Plan> P;
+    if (d.d1 * d.d2 * d.d3 > 0) {
+      P = d.plan_kind == T213_PLAN_AUTO ? group_plan(d.d1, d.d2, d.d3, d.elem_bytes, &rc) : nullptr;
+      if (!P) P = get_plan(d.d1, d.d2, d.d3, d.elem_bytes, d.plan_kind, 0, &rc);
+      if (!P) return fail(rc);
+      if (!plan_fits_batch(*P) || d.d1 * d.d2 * d.d3 * d.elem_bytes > direct_threshold()) B->spill.push_back(i);
+    }
+    B->plans.push_back(P);
+  }
+
+  BatchTables T;
+  {
+    std::vector<char> skip(count, 0);
+    for (int i : B->spill) skip[i] = 1;
+    if ((rc = build_batch_tables(tensors, count, B->plans, skip, T))) return fail(rc);
+  }
+  B->h_passes = std::move(T.passes);
+  B->h_items = std::move(T.items);
+  // carry pool
+  if (T.carry_bytes > 0) {
+    cudaError_t e = cudaMalloc(&B->d_carry, T.carry_bytes);
+    if (e != cudaSuccess) return fail(cuda_status(e, "batch carry pool"));
+    B->carry_bytes = T.carry_bytes;
+    bind_carry(B->h_passes, T.carry_off, B->d_carry);
+  }
+  B->n_ctrs = (int)B->h_passes.size();
 
   // ---- upload --------------------------------------------------------------
   cudaError_t e = cudaSuccess;

@@ -36,6 +36,8 @@ struct Plan {
 // Builds the plan of a family (T213_PLAN_*; AUTO picks).  t = 0 lets the
 // planner choose the block/band size.  Cached per device.
 std::shared_ptr<Plan> get_plan(int64_t d1, int64_t d2, int64_t d3, int eb, int kind, int64_t t, int *status);
+// Whether get_plan would find this exact key in the cache (nothing is built).
+bool plan_cached(int64_t d1, int64_t d2, int64_t d3, int eb, int kind, int64_t t);
 // Runs a plan on `data` (d1*d2*d3*eb bytes) on stream st.
 int run_plan(const Plan &p, char *data, cudaStream_t st, LaunchStats *ls);
 // Extra device memory a run of the plan needs beyond the tensor (carries and
@@ -47,5 +49,26 @@ std::shared_ptr<Plan> make_c2r_plan(int64_t d1, int64_t d2, int64_t d3, int eb, 
 std::shared_ptr<Plan> make_r2c_plan(int64_t d1, int64_t d2, int64_t d3, int eb, bool skinny, int *status);
 
 int64_t ext_gcd(int64_t a, int64_t b, int64_t *mmi);
+
+// ---- grouped launches of the persistent batch kernel (batch.cu) ----------------
+// A reusable executor: fixed device tables, carry pool and pinned staging, so
+// a group of small tensors is transposed by one k_batch launch without any
+// allocation at launch time.  Used by the serving loop.
+struct GroupExec;
+GroupExec *group_exec_create(int64_t max_passes, int64_t max_items, size_t carry_bytes, int *status);
+void group_exec_destroy(GroupExec *g);
+// The plan a tensor takes inside the persistent kernel (the automatic choice,
+// else another family whose passes fit its shared memory); null if none fits.
+std::shared_ptr<Plan> group_plan(int64_t d1, int64_t d2, int64_t d3, int eb, int *status);
+// Enqueues one k_batch launch over the tensors on st (tables copied from the
+// executor's pinned staging, counters reset), then copies the kernel's status
+// word to the executor's host mirror and records its event.  The executor's
+// previous launch must have finished (group_exec_idle).  Returns
+// T213_ERR_UNSUPPORTED, with nothing enqueued, when a tensor has no plan that
+// fits or the group exceeds the executor's capacity.
+int group_exec_run(GroupExec *g, const t213_tensor_desc *tensors, int32_t count, cudaStream_t st);
+bool group_exec_idle(GroupExec *g);
+// Status word of the last finished launch (0, or T213_ERR_TIMEOUT).
+int group_exec_status(GroupExec *g);
 
 }  // namespace t213

@@ -629,6 +629,12 @@ std::shared_ptr<Plan> new_plan(int64_t d1, int64_t d2, int64_t d3, int eb) {
 
 int tuner_lookup_internal(int64_t d1, int64_t d2, int64_t d3, int eb, int *kind, int64_t *t);
 
+bool plan_cached(int64_t d1, int64_t d2, int64_t d3, int eb, int kind, int64_t t) {
+  PlanKey key{d1, d2, d3, eb, kind, t, dev_info().id};
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  return g_plans.find(key) != g_plans.end();
+}
+
 std::shared_ptr<Plan> get_plan(int64_t d1, int64_t d2, int64_t d3, int eb, int kind, int64_t t, int *status) {
   *status = T213_OK;
   const int dev = dev_info().id;

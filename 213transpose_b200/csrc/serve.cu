@@ -42,28 +42,31 @@ __device__ __forceinline__ uint64_t fold(uint64_t w0, uint64_t w1, int eb) {
 
 __device__ __forceinline__ uint64_t term(uint64_t pos, uint64_t v) { return smix(pos * 0x100000001B3ull ^ v); }
 
-__global__ void k_fill(unsigned char *p, int64_t nel, int eb, uint64_t seed) {
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x) {
-    const uint64_t w0 = fill_word(seed, (uint64_t)e, 0);
-    switch (eb) {
-      case 1:
-        p[e] = (unsigned char)w0;
-        break;
-      case 2:
-        reinterpret_cast<uint16_t *>(p)[e] = (uint16_t)w0;
-        break;
-      case 4:
-        reinterpret_cast<uint32_t *>(p)[e] = (uint32_t)w0;
-        break;
-      case 8:
-        reinterpret_cast<unsigned long long *>(p)[e] = w0;
-        break;
-      default: {
-        const uint64_t w1 = fill_word(seed, (uint64_t)e, 1);
-        reinterpret_cast<uint4 *>(p)[e] = make_uint4((uint32_t)w0, (uint32_t)(w0 >> 32), (uint32_t)w1, (uint32_t)(w1 >> 32));
-      }
+__device__ __forceinline__ void fill_elem(unsigned char *p, int64_t e, int eb, uint64_t seed) {
+  const uint64_t w0 = fill_word(seed, (uint64_t)e, 0);
+  switch (eb) {
+    case 1:
+      p[e] = (unsigned char)w0;
+      break;
+    case 2:
+      reinterpret_cast<uint16_t *>(p)[e] = (uint16_t)w0;
+      break;
+    case 4:
+      reinterpret_cast<uint32_t *>(p)[e] = (uint32_t)w0;
+      break;
+    case 8:
+      reinterpret_cast<unsigned long long *>(p)[e] = w0;
+      break;
+    default: {
+      const uint64_t w1 = fill_word(seed, (uint64_t)e, 1);
+      reinterpret_cast<uint4 *>(p)[e] = make_uint4((uint32_t)w0, (uint32_t)(w0 >> 32), (uint32_t)w1, (uint32_t)(w1 >> 32));
     }
   }
+}
+
+__global__ void k_fill(unsigned char *p, int64_t nel, int eb, uint64_t seed) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x)
+    fill_elem(p, e, eb, seed);
 }
 
 __device__ __forceinline__ void reduce_add(uint64_t v, unsigned long long *out) {
@@ -71,32 +74,65 @@ __device__ __forceinline__ void reduce_add(uint64_t v, unsigned long long *out) 
   if ((threadIdx.x & 31) == 0) atomicAdd(out, (unsigned long long)v);
 }
 
+__device__ __forceinline__ uint64_t checksum_term(const unsigned char *p, int64_t e, int eb) {
+  uint64_t w0 = 0, w1 = 0;
+  switch (eb) {
+    case 1:
+      w0 = p[e];
+      break;
+    case 2:
+      w0 = reinterpret_cast<const uint16_t *>(p)[e];
+      break;
+    case 4:
+      w0 = reinterpret_cast<const uint32_t *>(p)[e];
+      break;
+    case 8:
+      w0 = reinterpret_cast<const unsigned long long *>(p)[e];
+      break;
+    default: {
+      const uint4 v = reinterpret_cast<const uint4 *>(p)[e];
+      w0 = (uint64_t)v.x | ((uint64_t)v.y << 32);
+      w1 = (uint64_t)v.z | ((uint64_t)v.w << 32);
+    }
+  }
+  return term((uint64_t)e, fold(w0, w1, eb));
+}
+
 __global__ void k_checksum(const unsigned char *p, int64_t nel, int eb, unsigned long long *out) {
   uint64_t acc = 0;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x) {
-    uint64_t w0 = 0, w1 = 0;
-    switch (eb) {
-      case 1:
-        w0 = p[e];
-        break;
-      case 2:
-        w0 = reinterpret_cast<const uint16_t *>(p)[e];
-        break;
-      case 4:
-        w0 = reinterpret_cast<const uint32_t *>(p)[e];
-        break;
-      case 8:
-        w0 = reinterpret_cast<const unsigned long long *>(p)[e];
-        break;
-      default: {
-        const uint4 v = reinterpret_cast<const uint4 *>(p)[e];
-        w0 = (uint64_t)v.x | ((uint64_t)v.y << 32);
-        w1 = (uint64_t)v.z | ((uint64_t)v.w << 32);
-      }
-    }
-    acc += term((uint64_t)e, fold(w0, w1, eb));
-  }
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nel; e += (int64_t)gridDim.x * blockDim.x)
+    acc += checksum_term(p, e, eb);
   reduce_add(acc, out);
+}
+
+// A group of requests handled by one launch each of fill, transpose
+// (k_batch) and checksum: blockIdx.y picks the request.
+constexpr int kMaxGroup = 64;
+struct GroupReq {
+  unsigned char *p;
+  int64_t nel;
+  uint64_t seed;
+  int32_t eb, pad;
+};
+struct GroupArgs {
+  GroupReq r[kMaxGroup];
+};
+
+// also zeroes the request's checksum accumulator (read by k_checksum_group,
+// which runs after the transpose on the same stream)
+__global__ void k_fill_group(const GroupArgs a, unsigned long long *sums) {
+  const GroupReq R = a.r[blockIdx.y];
+  if (blockIdx.x == 0 && threadIdx.x == 0) sums[blockIdx.y] = 0;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < R.nel; e += (int64_t)gridDim.x * blockDim.x)
+    fill_elem(R.p, e, R.eb, R.seed);
+}
+
+__global__ void k_checksum_group(const GroupArgs a, unsigned long long *sums) {
+  const GroupReq R = a.r[blockIdx.y];
+  uint64_t acc = 0;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < R.nel; e += (int64_t)gridDim.x * blockDim.x)
+    acc += checksum_term(R.p, e, R.eb);
+  reduce_add(acc, sums + blockIdx.y);
 }
 
 // Checksum a correct 213 transpose must have: output position o holds the
@@ -171,6 +207,16 @@ int grid_for(int64_t nel) {
 
 using namespace t213;
 
+// One grouped launch in flight: its executor (tables, k_batch), the
+// checksums of its requests and the event after their copies.
+struct ServeGroup {
+  GroupExec *ex = nullptr;
+  unsigned long long *d_sums = nullptr;
+  unsigned long long *h_sums = nullptr;  // pinned
+  cudaEvent_t ev = nullptr;
+  int pending = 0;  // requests of the last launch not yet completed
+};
+
 struct t213_server_st {
   int dev = 0;
   char *arena = nullptr;
@@ -181,6 +227,8 @@ struct t213_server_st {
   unsigned long long *h_sums = nullptr;  // pinned mirror
   std::vector<cudaEvent_t> events;
   Arena arena_map;
+  std::vector<ServeGroup> groups;
+  int64_t group_max_bytes = 0;  // requests up to this size may share a launch
 };
 
 namespace {
@@ -188,9 +236,20 @@ namespace {
 struct Slot {
   int req = -1;
   int64_t off = 0, bytes = 0;
+  cudaEvent_t ev = nullptr;                 // completion of the request
+  const unsigned long long *sum = nullptr;  // its checksum, valid after ev
+  int group = -1;                           // the ServeGroup it ran in
 };
 
-int enqueue_request(t213_server s, const t213_request &r, int slot, int64_t off, cudaStream_t st) {
+// Copies a finished request's tensor out to the caller's buffer (stream
+// ordered, before the completion event).
+int enqueue_capture(void *out, const void *p, int64_t bytes, cudaStream_t st) {
+  if (!out) return T213_OK;
+  cudaError_t e = cudaMemcpyAsync(out, p, (size_t)bytes, cudaMemcpyDeviceToHost, st);
+  return e == cudaSuccess ? T213_OK : cuda_status(e, "result copy");
+}
+
+int enqueue_request(t213_server s, const t213_request &r, int slot, int64_t off, cudaStream_t st, void *capture) {
   const int64_t nel = r.d1 * r.d2 * r.d3;
   unsigned char *p = (unsigned char *)s->arena + off;
   k_fill<<<grid_for(nel), 256, 0, st>>>(p, nel, r.elem_bytes, r.seed);
@@ -201,22 +260,85 @@ int enqueue_request(t213_server s, const t213_request &r, int slot, int64_t off,
   cudaMemsetAsync(s->d_sums + slot, 0, sizeof(unsigned long long), st);
   k_checksum<<<grid_for(nel), 256, 0, st>>>(p, nel, r.elem_bytes, s->d_sums + slot);
   cudaMemcpyAsync(s->h_sums + slot, s->d_sums + slot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+  if ((rc = enqueue_capture(capture, p, nel * r.elem_bytes, st))) return rc;
   cudaError_t e = cudaEventRecord(s->events[slot], st);
   if (e != cudaSuccess) return cuda_status(e, "cudaEventRecord");
   e = cudaGetLastError();
   return e == cudaSuccess ? T213_OK : cuda_status(e, "request launch");
 }
 
+// Several admitted requests in one launch of each kind: a grouped fill, one
+// persistent k_batch over all their transposes, a grouped checksum.
+// T213_ERR_UNSUPPORTED if the executor cannot take them; the grouped fill
+// has been enqueued then, and the caller runs the requests one by one.
+int enqueue_group(t213_server s, ServeGroup &G, const t213_request *reqs, const std::vector<int> &slot_ids,
+                  std::vector<Slot> &slots, cudaStream_t st, void *const *capture) {
+  const int n = (int)slot_ids.size();
+  GroupArgs a{};
+  std::vector<t213_tensor_desc> descs(n);
+  int64_t max_nel = 0;
+  for (int r = 0; r < n; r++) {
+    const Slot &S = slots[slot_ids[r]];
+    const t213_request &q = reqs[S.req];
+    unsigned char *p = (unsigned char *)s->arena + S.off;
+    a.r[r] = GroupReq{p, q.d1 * q.d2 * q.d3, q.seed, q.elem_bytes, 0};
+    descs[r] = t213_tensor_desc{p, q.d1, q.d2, q.d3, q.elem_bytes, T213_PLAN_AUTO};
+    max_nel = std::max(max_nel, q.d1 * q.d2 * q.d3);
+  }
+  const int gx = (int)std::max<int64_t>(
+      1, std::min<int64_t>((max_nel + 255) / 256, std::max<int64_t>(1, (int64_t)dev_info().sms * 8 / n)));
+  k_fill_group<<<dim3(gx, n), 256, 0, st>>>(a, G.d_sums);
+  int rc = group_exec_run(G.ex, descs.data(), n, st);
+  if (rc) return rc;
+  k_checksum_group<<<dim3(gx, n), 256, 0, st>>>(a, G.d_sums);
+  cudaError_t e = cudaMemcpyAsync(G.h_sums, G.d_sums, n * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+  if (e != cudaSuccess) return cuda_status(e, "group checksums");
+  for (int r = 0; r < n; r++) {
+    const Slot &S = slots[slot_ids[r]];
+    if (capture && capture[S.req] && (rc = enqueue_capture(capture[S.req], a.r[r].p, a.r[r].nel * a.r[r].eb, st)))
+      return rc;
+  }
+  e = cudaEventRecord(G.ev, st);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_status(e, "group launch");
+  for (int r = 0; r < n; r++) {
+    Slot &S = slots[slot_ids[r]];
+    S.ev = G.ev;
+    S.sum = G.h_sums + r;
+    S.group = (int)(&G - s->groups.data());
+  }
+  G.pending = n;
+  return T213_OK;
+}
+
+// Requests run one by one, each on the stream with its own event and checksum.
+int enqueue_singles(t213_server s, const t213_request *reqs, const std::vector<int> &slot_ids,
+                    std::vector<Slot> &slots, cudaStream_t st, void *const *capture) {
+  for (int sl : slot_ids) {
+    Slot &S = slots[sl];
+    int rc = enqueue_request(s, reqs[S.req], sl, S.off, st, capture ? capture[S.req] : nullptr);
+    if (rc) return rc;
+    S.ev = s->events[sl];
+    S.sum = s->h_sums + sl;
+    S.group = -1;
+  }
+  return T213_OK;
+}
+
 // Plans requests on worker threads as they arrive, so that the dispatch loop
 // only looks plans up: building a new shape's plan (its cycle tables above
 // all) takes from microseconds to tens of milliseconds of host time, which a
-// single dispatch thread would otherwise spend while the GPU idles.
+// single dispatch thread would otherwise spend while the GPU idles.  For a
+// request small enough to share a launch it also finds the plan the
+// persistent kernel would run, and it notes whether the request's shape had
+// to be planned (a cold request) or was found in the plan cache (warm).
 class PlannerPool {
  public:
-  PlannerPool(int dev, int threads, const t213_request *reqs, int n) : reqs_(reqs), planned_(n) {
+  PlannerPool(int dev, int threads, const t213_request *reqs, int n, int64_t group_max_bytes)
+      : reqs_(reqs), planned_(n), groupable_(n, 0), cold_(n, 0) {
     for (auto &f : planned_) f.store(0, std::memory_order_relaxed);
     for (int i = 0; i < threads; i++)
-      workers_.emplace_back([this, dev] {
+      workers_.emplace_back([this, dev, group_max_bytes] {
         cudaSetDevice(dev);
         for (;;) {
           int ri;
@@ -230,8 +352,14 @@ class PlannerPool {
           const t213_request &r = reqs_[ri];
           int st = T213_OK;
           if (r.d1 > 0 && r.d2 > 0 && r.d3 > 0 &&
-              (r.elem_bytes == 1 || r.elem_bytes == 2 || r.elem_bytes == 4 || r.elem_bytes == 8 || r.elem_bytes == 16))
+              (r.elem_bytes == 1 || r.elem_bytes == 2 || r.elem_bytes == 4 || r.elem_bytes == 8 ||
+               r.elem_bytes == 16)) {
+            cold_[ri] = !plan_cached(r.d1, r.d2, r.d3, r.elem_bytes, r.plan_kind, 0);
             get_plan(r.d1, r.d2, r.d3, r.elem_bytes, r.plan_kind, 0, &st);  // errors resurface at dispatch
+            const int64_t bytes = r.d1 * r.d2 * r.d3 * r.elem_bytes;
+            if (r.plan_kind == T213_PLAN_AUTO && bytes <= group_max_bytes)
+              groupable_[ri] = group_plan(r.d1, r.d2, r.d3, r.elem_bytes, &st) != nullptr;
+          }
           planned_[ri].store(1, std::memory_order_release);
         }
       });
@@ -253,10 +381,14 @@ class PlannerPool {
     cv_.notify_one();
   }
   bool ready(int ri) const { return planned_[ri].load(std::memory_order_acquire) != 0; }
+  // valid once ready(ri)
+  bool groupable(int ri) const { return groupable_[ri] != 0; }
+  bool cold(int ri) const { return cold_[ri] != 0; }
 
  private:
   const t213_request *reqs_;
   std::vector<std::atomic<int>> planned_;
+  std::vector<char> groupable_, cold_;  // written by one worker before planned_ is released
   std::vector<std::thread> workers_;
   std::mutex mu_;
   std::condition_variable cv_;
@@ -271,6 +403,13 @@ int planner_threads() {
   if (v && std::atoi(v) > 0) return std::min(64, std::atoi(v));
   const int hw = (int)std::thread::hardware_concurrency();
   return std::max(1, std::min(16, hw - 2));
+}
+
+double percentile(std::vector<double> v, double p) {
+  if (v.empty()) return 0.0;
+  std::sort(v.begin(), v.end());
+  size_t k = (size_t)std::min<double>((double)v.size() - 1, std::ceil(p * v.size()) - 1);
+  return v[k];
 }
 
 }  // namespace
@@ -292,7 +431,14 @@ int t213_server_create(int64_t hbm_budget_bytes, int32_t max_inflight, int32_t n
     delete s;
     return cuda_status(e, "cudaMemGetInfo");
   }
-  const int64_t margin = (int64_t)2 << 30;
+  // grouped launches: T213_SERVE_GROUPS executors (default 4, 0 = off) for
+  // requests of at most T213_SERVE_GROUP_MB (default 32)
+  const char *gv = std::getenv("T213_SERVE_GROUPS");
+  const int n_groups = gv ? std::max(0, std::min(16, std::atoi(gv))) : 4;
+  const char *gm = std::getenv("T213_SERVE_GROUP_MB");
+  s->group_max_bytes = n_groups ? (int64_t)((gm ? atof(gm) : 32.0) * (1 << 20)) : 0;
+  const size_t group_carry = (size_t)64 << 20;
+  const int64_t margin = ((int64_t)2 << 30) + n_groups * (int64_t)(group_carry + (8 << 20));
   s->arena_bytes = std::min<int64_t>(hbm_budget_bytes, (int64_t)free_b - margin);
   if (s->arena_bytes <= 0) {
     delete s;
@@ -323,12 +469,24 @@ int t213_server_create(int64_t hbm_budget_bytes, int32_t max_inflight, int32_t n
     if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming))) return fail(e, "event");
     s->events.push_back(ev);
   }
+  s->groups.resize(n_groups);
+  for (ServeGroup &G : s->groups) {
+    int rc = T213_OK;
+    G.ex = group_exec_create(1024, 1 << 16, group_carry, &rc);
+    if (!G.ex) {
+      t213_server_destroy(s);
+      return rc;
+    }
+    if ((e = cudaMalloc(&G.d_sums, sizeof(unsigned long long) * kMaxGroup))) return fail(e, "group sums");
+    if ((e = cudaMallocHost(&G.h_sums, sizeof(unsigned long long) * kMaxGroup))) return fail(e, "group sums");
+    if ((e = cudaEventCreateWithFlags(&G.ev, cudaEventDisableTiming))) return fail(e, "group event");
+  }
   *out = s;
   return T213_OK;
 }
 
-int t213_server_run(t213_server s, const t213_request *reqs, int32_t n, t213_serve_stats *stats, uint64_t *checksums,
-                    double *latency_ms) {
+int t213_server_run_capture(t213_server s, const t213_request *reqs, int32_t n, t213_serve_stats *stats,
+                            uint64_t *checksums, double *latency_ms, void *const *outputs) {
   if (!s || n < 0 || (n > 0 && !reqs)) return T213_ERR_INVALID_ARGUMENT;
   using clk = std::chrono::steady_clock;
   std::vector<int> order(n);
@@ -341,10 +499,31 @@ int t213_server_run(t213_server s, const t213_request *reqs, int32_t n, t213_ser
   std::vector<int> free_slots;
   for (int i = s->max_inflight - 1; i >= 0; i--) free_slots.push_back(i);
   int next = 0, done = 0, rejected = 0, rr = 0;
-  int64_t bytes_done = 0, peak = 0, max_inflight = 0, inflight = 0;
-  PlannerPool planners(s->dev, planner_threads(), reqs, n);
+  int64_t bytes_done = 0, peak = 0, max_inflight = 0, inflight = 0, group_launches = 0, grouped = 0;
+  PlannerPool planners(s->dev, planner_threads(), reqs, n, s->group_max_bytes);
   const auto t0 = clk::now();
   auto now_s = [&]() { return std::chrono::duration<double>(clk::now() - t0).count(); };
+  std::vector<int> grp;  // slots admitted in this round that may share a launch
+  auto flush_group = [&]() -> int {
+    if (grp.empty()) return T213_OK;
+    cudaStream_t st = s->streams[rr++ % s->streams.size()];
+    ServeGroup *G = nullptr;
+    if (grp.size() >= 2)
+      for (ServeGroup &g : s->groups)
+        if (g.pending == 0 && group_exec_idle(g.ex)) {
+          G = &g;
+          break;
+        }
+    int rc = G ? enqueue_group(s, *G, reqs, grp, slots, st, outputs) : T213_ERR_UNSUPPORTED;
+    if (rc == T213_OK) {
+      group_launches++;
+      grouped += (int64_t)grp.size();
+    } else if (rc == T213_ERR_UNSUPPORTED) {
+      rc = enqueue_singles(s, reqs, grp, slots, st, outputs);
+    }
+    grp.clear();
+    return rc;
+  };
   while (done + rejected < n) {
     bool progress = false;
     const double t = now_s();
@@ -356,14 +535,22 @@ int t213_server_run(t213_server s, const t213_request *reqs, int32_t n, t213_ser
     for (int sl = 0; sl < s->max_inflight; sl++) {
       Slot &S = slots[sl];
       if (S.req < 0) continue;
-      cudaError_t q = cudaEventQuery(s->events[sl]);
+      cudaError_t q = cudaEventQuery(S.ev);
       if (q == cudaErrorNotReady) continue;
       if (q != cudaSuccess) return cuda_status(q, "request completion");
+      if (S.group >= 0) {
+        ServeGroup &G = s->groups[S.group];
+        if (group_exec_status(G.ex)) {
+          set_error("a bounded wait of a grouped serving launch ran out");
+          return T213_ERR_TIMEOUT;
+        }
+        G.pending--;
+      }
       lat[S.req] = (now_s() - reqs[S.req].arrival_s) * 1e3;
-      sums[S.req] = s->h_sums[sl];
+      sums[S.req] = *S.sum;
       bytes_done += S.bytes;
       s->arena_map.release(S.off, S.bytes);
-      S.req = -1;
+      S = Slot{};
       free_slots.push_back(sl);
       inflight--;
       done++;
@@ -372,7 +559,8 @@ int t213_server_run(t213_server s, const t213_request *reqs, int32_t n, t213_ser
     // admissions in arrival order among the requests whose plans are ready
     // (a request still being planned is passed over, not waited for; the
     // first one that does not fit the arena stops admission until memory
-    // frees up, so large requests are not starved)
+    // frees up, so large requests are not starved).  Small requests admitted
+    // in the same round share one launch of each kernel.
     size_t pi = 0;
     while (pi < pending.size() && pi < 256 && !free_slots.empty()) {
       const int ri = pending[pi];
@@ -400,14 +588,28 @@ int t213_server_run(t213_server s, const t213_request *reqs, int32_t n, t213_ser
       pending.erase(pending.begin() + pi);
       const int sl = free_slots.back();
       free_slots.pop_back();
-      slots[sl] = Slot{ri, off, bytes};
-      cudaStream_t st = s->streams[rr++ % s->streams.size()];
-      int rc = enqueue_request(s, r, sl, off, st);
-      if (rc) return rc;
+      slots[sl] = Slot{ri, off, bytes, nullptr, nullptr, -1};
       inflight++;
       max_inflight = std::max(max_inflight, inflight);
       peak = std::max(peak, s->arena_map.used());
       progress = true;
+      if (!s->groups.empty() && planners.groupable(ri)) {
+        grp.push_back(sl);
+        if ((int)grp.size() == kMaxGroup) {
+          int rc = flush_group();
+          if (rc) return rc;
+        }
+        continue;
+      }
+      cudaStream_t st = s->streams[rr++ % s->streams.size()];
+      int rc = enqueue_request(s, r, sl, off, st, outputs ? outputs[ri] : nullptr);
+      if (rc) return rc;
+      slots[sl].ev = s->events[sl];
+      slots[sl].sum = s->h_sums + sl;
+    }
+    {
+      int rc = flush_group();
+      if (rc) return rc;
     }
     if (!progress) {
       // nothing to do until the next arrival or completion
@@ -419,32 +621,42 @@ int t213_server_run(t213_server s, const t213_request *reqs, int32_t n, t213_ser
     }
   }
   const double wall = now_s();
-  std::vector<double> ok;
+  std::vector<double> ok, cold, warm;
   for (int i = 0; i < n; i++)
-    if (lat[i] >= 0) ok.push_back(lat[i]);
-  std::sort(ok.begin(), ok.end());
-  auto pct = [&](double p) {
-    if (ok.empty()) return 0.0;
-    size_t k = (size_t)std::min<double>((double)ok.size() - 1, std::ceil(p * ok.size()) - 1);
-    return ok[k];
-  };
+    if (lat[i] >= 0) {
+      ok.push_back(lat[i]);
+      (planners.cold(i) ? cold : warm).push_back(lat[i]);
+    }
   if (stats) {
+    *stats = t213_serve_stats{};
     stats->completed = done;
     stats->rejected = rejected;
     stats->bytes_done = bytes_done;
-    stats->p50_ms = pct(0.50);
-    stats->p99_ms = pct(0.99);
+    stats->p50_ms = percentile(ok, 0.50);
+    stats->p99_ms = percentile(ok, 0.99);
     double sum = 0;
     for (double v : ok) sum += v;
     stats->mean_ms = ok.empty() ? 0 : sum / ok.size();
-    stats->max_ms = ok.empty() ? 0 : ok.back();
+    stats->max_ms = ok.empty() ? 0 : *std::max_element(ok.begin(), ok.end());
     stats->wall_s = wall;
     stats->peak_resident_bytes = peak;
     stats->max_inflight = max_inflight;
+    stats->cold = (int64_t)cold.size();
+    stats->p50_cold_ms = percentile(cold, 0.50);
+    stats->p99_cold_ms = percentile(cold, 0.99);
+    stats->p50_warm_ms = percentile(warm, 0.50);
+    stats->p99_warm_ms = percentile(warm, 0.99);
+    stats->group_launches = group_launches;
+    stats->grouped_requests = grouped;
   }
   if (checksums) std::copy(sums.begin(), sums.end(), checksums);
   if (latency_ms) std::copy(lat.begin(), lat.end(), latency_ms);
   return T213_OK;
+}
+
+int t213_server_run(t213_server s, const t213_request *reqs, int32_t n, t213_serve_stats *stats, uint64_t *checksums,
+                    double *latency_ms) {
+  return t213_server_run_capture(s, reqs, n, stats, checksums, latency_ms, nullptr);
 }
 
 int t213_server_expected_checksum(t213_server s, const t213_request *r, uint64_t *checksum) {
@@ -469,7 +681,7 @@ int t213_server_run_alone(t213_server s, const t213_request *r, uint64_t *checks
   }
   const int64_t off = s->arena_map.alloc(bytes);
   if (off < 0) return T213_ERR_BUDGET;
-  int rc = enqueue_request(s, *r, 0, off, s->streams[0]);
+  int rc = enqueue_request(s, *r, 0, off, s->streams[0], nullptr);
   cudaError_t e = cudaStreamSynchronize(s->streams[0]);
   s->arena_map.release(off, bytes);
   if (rc) return rc;
@@ -482,6 +694,12 @@ int t213_server_destroy(t213_server s) {
   if (!s) return T213_OK;
   for (cudaStream_t st : s->streams) cudaStreamSynchronize(st);
   for (cudaEvent_t ev : s->events) cudaEventDestroy(ev);
+  for (ServeGroup &G : s->groups) {
+    group_exec_destroy(G.ex);
+    if (G.ev) cudaEventDestroy(G.ev);
+    if (G.d_sums) cudaFree(G.d_sums);
+    if (G.h_sums) cudaFreeHost(G.h_sums);
+  }
   for (cudaStream_t st : s->streams) {
     release_stream_workspace(st);
     cudaStreamDestroy(st);

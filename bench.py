@@ -465,6 +465,10 @@ def serving_section(t213, torch):
             "completed": stats["completed"], "rejected": stats["rejected"],
             "p50_ms": round(stats["p50_ms"], 3), "p99_ms": round(stats["p99_ms"], 3),
             "mean_ms": round(stats["mean_ms"], 3), "max_ms": round(stats["max_ms"], 3),
+            "cold_requests": stats["cold"], "p50_cold_ms": round(stats["p50_cold_ms"], 3),
+            "p99_cold_ms": round(stats["p99_cold_ms"], 3), "p50_warm_ms": round(stats["p50_warm_ms"], 3),
+            "p99_warm_ms": round(stats["p99_warm_ms"], 3),
+            "group_launches": stats["group_launches"], "grouped_requests": stats["grouped_requests"],
             "throughput_GBps": round(stats["bytes_done"] / stats["wall_s"] / 1e9, 2),
             "requests_per_s": round(stats["completed"] / stats["wall_s"], 1),
             "peak_resident_GB": round(stats["peak_resident_bytes"] / 1e9, 2),

@@ -13,8 +13,12 @@
  * for the producer), transposed in place on one of the server's streams, and
  * checksummed.  Admitted requests run concurrently on the stream pool while new
  * ones keep arriving and being admitted as memory and slots free up
- * (continuous batching).  Latency is measured on the host from the scheduled
- * arrival to the detected completion of the transpose.
+ * (continuous batching).  Small requests (T213_SERVE_GROUP_MB, default 32 MB)
+ * admitted together share launches: one grouped fill, one persistent batch
+ * kernel over all their transposes (the executor of the batched form) and one
+ * grouped checksum, on T213_SERVE_GROUPS (default 4) reusable executors.
+ * Latency is measured on the host from the scheduled arrival to the detected
+ * completion of the transpose.
  */
 #ifndef T213_SERVE_H
 #define T213_SERVE_H
@@ -39,6 +43,13 @@ typedef struct t213_serve_stats {
   int64_t completed, rejected, bytes_done;
   double p50_ms, p99_ms, mean_ms, max_ms, wall_s;
   int64_t peak_resident_bytes, max_inflight;
+  /* cold: requests whose shape was not in the plan cache when they arrived
+   * (they waited for planning); warm: the others */
+  int64_t cold;
+  double p50_cold_ms, p99_cold_ms, p50_warm_ms, p99_warm_ms;
+  /* launches of the persistent kernel over several small requests, and the
+   * requests they carried */
+  int64_t group_launches, grouped_requests;
 } t213_serve_stats;
 
 typedef struct t213_server_st *t213_server;
@@ -52,6 +63,11 @@ int t213_server_create(int64_t hbm_budget_bytes, int32_t max_inflight, int32_t n
  * (optional, n entries) receives each request's latency (-1 if rejected). */
 int t213_server_run(t213_server s, const t213_request *requests, int32_t n, t213_serve_stats *stats,
                     uint64_t *checksums, double *latency_ms);
+/* The same, and for every request whose outputs[i] is not NULL the transposed
+ * tensor is copied there (d1*d2*d3*elem_bytes bytes of host memory, pinned
+ * for an asynchronous copy) before the request counts as complete. */
+int t213_server_run_capture(t213_server s, const t213_request *requests, int32_t n, t213_serve_stats *stats,
+                            uint64_t *checksums, double *latency_ms, void *const *outputs);
 
 /* The checksum a correct transpose of the request's tensor has, computed on
  * the device from the fill without transposing anything. */
