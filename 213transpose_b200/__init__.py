@@ -9,9 +9,9 @@ from ._lib import T213Error, lib, header_functions, SO_PATH  # noqa: F401
 from .api import (inplace, transpose, c2r_transpose, r2c_transpose, skinny_c2r_transpose,  # noqa: F401
                   skinny_r2c_transpose, rotate, shuffle_fn, col_shuffle_fn, scatter_permute, permute,
                   transpose_with_plan, transpose_host, describe, plan_launches, pass_timing,
-                  release_cache, Batch, Server, device_status)
+                  release_cache, Batch, Server, device_status, tuner)
 
 __all__ = ["inplace", "transpose", "c2r_transpose", "r2c_transpose", "skinny_c2r_transpose",
            "skinny_r2c_transpose", "rotate", "shuffle_fn", "col_shuffle_fn", "scatter_permute", "permute",
            "transpose_with_plan", "transpose_host", "describe", "plan_launches", "pass_timing",
-           "release_cache", "Batch", "Server", "device_status", "T213Error", "lib"]
+           "release_cache", "Batch", "Server", "device_status", "tuner", "T213Error", "lib"]

@@ -217,6 +217,51 @@ class pass_timing:
         return ms.value, n.value
 
 
+class _Tuner:
+    """The autotuner (t213_tune_shape, t213_tuner_*): per shape it times the
+    applicable plan families, the winner's block or band size and the kernel
+    variants of its passes, and caches the winner per exact shape and per
+    shape class; the automatic plan choice (plan="auto") then uses it."""
+
+    @staticmethod
+    def tune(d1, d2, d3, elem_bytes, scratch=None, stream=None):
+        """Tunes one shape on a scratch device buffer of the tensor's size
+        (allocated here when not given); returns (plan name, block size)."""
+        torch = _t()
+        buf = scratch if scratch is not None else torch.empty(int(d1) * int(d2) * int(d3) * int(elem_bytes),
+                                                              dtype=torch.uint8, device="cuda")
+        kind, t = ctypes.c_int32(0), ctypes.c_int64(0)
+        check(lib().t213_tune_shape(ctypes.c_void_p(buf.data_ptr()), int(d1), int(d2), int(d3), int(elem_bytes),
+                                    _stream_of(stream), ctypes.byref(kind), ctypes.byref(t)))
+        names = {v: k for k, v in _lib.PLAN_NAMES.items()}
+        return names[int(kind.value)], int(t.value)
+
+    @staticmethod
+    def lookup(d1, d2, d3, elem_bytes):
+        """(plan name, block size) cached for the shape, or None."""
+        kind, t = ctypes.c_int32(0), ctypes.c_int64(0)
+        rc = lib().t213_tuner_lookup(int(d1), int(d2), int(d3), int(elem_bytes), ctypes.byref(kind), ctypes.byref(t))
+        if rc != _lib.OK:
+            return None
+        names = {v: k for k, v in _lib.PLAN_NAMES.items()}
+        return names[int(kind.value)], int(t.value)
+
+    @staticmethod
+    def save(path):
+        check(lib().t213_tuner_save(str(path).encode()))
+
+    @staticmethod
+    def load(path):
+        check(lib().t213_tuner_load(str(path).encode()))
+
+    @staticmethod
+    def clear():
+        check(lib().t213_tuner_clear())
+
+
+tuner = _Tuner()
+
+
 class Batch:
     """Many tensors transposed by one persistent, graph-captured launch
     (t213_batch_*).  `tensors` is a list of (data, d1, d2, d3) or

@@ -103,6 +103,33 @@ struct LaunchStats {
   int launches = 0;
 };
 
+// Kernel choices a plan may pin; 0 leaves a launcher's default (its
+// environment override, else its built-in rule).  The autotuner searches them
+// per shape class.
+struct Variant {
+  int8_t col = 0;   // column passes: 1 staged strips (no cluster-local form), 2 cluster-local 256-byte strips
+  int8_t row = 0;   // row passes: 1 staged rows, 2 double-buffered rows (k_row_pipe)
+  int8_t tile = 0;  // tile swaps: 1 TMA ring, 2 register tiles (k_tile_swap_vec)
+  int8_t seg = 0;   // segment cycles: 1 bulk walker ring of 6, 2 ring of 10, 3 register walker
+  bool any() const { return col || row || tile || seg; }
+  int packed() const { return (col & 15) | (row & 15) << 4 | (tile & 15) << 8 | (seg & 15) << 12; }
+  static Variant unpack(int v) {
+    Variant x;
+    x.col = (int8_t)(v & 15);
+    x.row = (int8_t)(v >> 4 & 15);
+    x.tile = (int8_t)(v >> 8 & 15);
+    x.seg = (int8_t)(v >> 12 & 15);
+    return x;
+  }
+};
+// The variant of the plan this host thread is launching (set by run_plan).
+const Variant &current_variant();
+struct VariantScope {
+  explicit VariantScope(const Variant &v);
+  ~VariantScope();
+  Variant saved;
+};
+
 // Column gather new[i][j] = old[f(i,j)][j] over d3 slices of m x n.
 int launch_col_gather(const FnSpec &f, char *data, int64_t d3, int64_t m, int64_t n, int eb,
                       cudaStream_t st, LaunchStats *ls);

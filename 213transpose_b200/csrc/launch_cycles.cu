@@ -318,14 +318,16 @@ int launch_seg_cycles(const CycleTable &ct, char *data, int64_t d3, int64_t slic
   // against 1.967 ms register; 480-byte (BANDS_T of (552630, 125, 1) 16-byte)
   // 0.555 against 1.160 ms.
   const char *bm = std::getenv("T213_SEG_BULK_MIN");
-  const int64_t bulk_min = bm && std::atoi(bm) >= 16 ? std::atoi(bm) : 256;
+  const Variant &pin = current_variant();
+  const int64_t bulk_min =
+      pin.seg == 3 ? INT64_MAX : pin.seg ? 256 : (bm && std::atoi(bm) >= 16 ? std::atoi(bm) : 256);
   if (aw == 16 && seg_bytes >= bulk_min) {
     // TMA bulk walker: pieces of up to 16 KB (T213_SEG_PIECE_KB), a ring of
     // 6 buffers (T213_SEG_RING=10 for 10)
     const char *pv = std::getenv("T213_SEG_PIECE_KB");
     const int64_t piece_cap = (pv && std::atoi(pv) > 0 ? std::atoi(pv) : 16) * 1024;
     const char *rv = std::getenv("T213_SEG_RING");
-    const int ring = (rv && std::atoi(rv) == 10) ? 10 : kBulkRing;
+    const int ring = pin.seg == 2 ? 10 : pin.seg == 1 ? kBulkRing : (rv && std::atoi(rv) == 10) ? 10 : kBulkRing;
     const int64_t piece = std::min<int64_t>(seg_bytes, piece_cap);
     const int64_t npieces = (seg_bytes + piece - 1) / piece;
     const int64_t smem = 128 + (int64_t)ring * piece;

@@ -262,7 +262,8 @@ bool local_params_ok(const FnSpec &f, int64_t m) {
 LocalCfg local_col_config(const FnSpec &f, int64_t m, int64_t n, int eb, const void *data) {
   LocalCfg c;
   const char *var = std::getenv("T213_COL_VARIANT");
-  if (var && std::strcmp(var, "old") == 0) return c;
+  const Variant &pv = current_variant();
+  if (pv.col == 1 || (pv.col == 0 && var && std::strcmp(var, "old") == 0)) return c;
   if (!local_form(f.kind) || m <= 0 || n <= 0 || !local_params_ok(f, m)) return c;
   c.aw = pick_aw(eb, data, n * eb, 0);
   const int64_t P = c.aw / eb;
@@ -277,7 +278,7 @@ LocalCfg local_col_config(const FnSpec &f, int64_t m, int64_t n, int eb, const v
   // (below a * a with a = m / gcd)
   c.u64 = !fits32(f, m, n) || (double)m * (double)m >= 2.0e9;
   const int64_t whole_cap = (env_int("T213_COL_WHOLE_KB") > 0 ? env_int("T213_COL_WHOLE_KB") : 104) * 1024;
-  if (m * 128 <= whole_cap && env_int("T213_COL_LOCAL_K") <= 1) {
+  if (m * 128 <= whole_cap && env_int("T213_COL_LOCAL_K") <= 1 && pv.col != 2) {
     // whole strips in one CTA: at least 128-byte rows, widened to about
     // 48 KB per strip (at most 256 columns), no halo
     c.W = width(std::max<int64_t>(128, (48 * 1024) / m));
@@ -300,6 +301,8 @@ LocalCfg local_col_config(const FnSpec &f, int64_t m, int64_t n, int eb, const v
   if (env_int("T213_COL_LOCAL_WBYTES") > 0 || env_int("T213_COL_LOCAL_SMEM_KB") > 0)
     tries.push_back({env_int("T213_COL_LOCAL_WBYTES") > 0 ? env_int("T213_COL_LOCAL_WBYTES") : 128,
                      env_int("T213_COL_LOCAL_SMEM_KB") > 0 ? env_int("T213_COL_LOCAL_SMEM_KB") : 100});
+  else if (pv.col == 2)  // 256-byte strips: longer DRAM bursts, fewer CTAs per SM
+    tries = {{256, 110}, {256, 200}, {128, 100}, {128, 200}, {64, 200}, {32, 200}, {16, 200}};
   else
     tries = {{128, 100}, {128, 200}, {64, 200}, {32, 200}, {16, 200}};
   for (const Try &t : tries) {
@@ -345,9 +348,11 @@ RowCfg row_config(int64_t m, int64_t n, int eb, const void *data) {
   // 2) C2R shuffle 0.345 ms staged against 0.388 ms double-buffered; R2C
   // shuffle 0.291 against 0.284 ms; fp32 (8192, 6143, 2) 0.212 against 0.209).
   const char *var = std::getenv("T213_ROW_VARIANT");
+  const Variant &pv = current_variant();
   const int64_t stage = (env_int("T213_ROW_STAGE_KB") > 0 ? env_int("T213_ROW_STAGE_KB") : 48) * 1024;
   const int64_t cap = std::max<int64_t>(stage, (kSmemCap / 2) / 16 * 16);
-  if (var && std::strcmp(var, "pipe") == 0 && row_bytes <= cap) {
+  const bool pipe = pv.row == 2 || (pv.row == 0 && var && std::strcmp(var, "pipe") == 0);
+  if (pipe && row_bytes <= cap) {
     r.K = 1;
     r.pipe = true;
     r.rows_per_unit = (int)std::max<int64_t>(1, std::min<int64_t>(m, stage / row_bytes));

@@ -47,6 +47,9 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 // T213_TILE_WARPS (consumer warps), T213_TILE_TS (tile side) and
 // T213_TILE_GROUP (super-tile order) set the TMA kernel's launch shape.
 const char *tile_swap_choice() {
+  const Variant &pv = current_variant();
+  if (pv.tile == 1) return "tma";
+  if (pv.tile == 2) return "vec";
   const char *v = std::getenv("T213_TILE_SWAP");
   return v ? v : "auto";
 }

@@ -31,11 +31,16 @@ struct Plan {
   std::vector<PassDesc> passes;
   std::string desc;
   double est_cost = 0;  // heuristic, in units of one full read+write sweep
+  Variant var;          // kernel choices pinned by the tuner (default: none)
 };
 
 // Builds the plan of a family (T213_PLAN_*; AUTO picks).  t = 0 lets the
 // planner choose the block/band size.  Cached per device.
 std::shared_ptr<Plan> get_plan(int64_t d1, int64_t d2, int64_t d3, int eb, int kind, int64_t t, int *status);
+// The plan of a family and block size with kernel variants pinned (a cached
+// copy of get_plan's plan); the plain plan when v pins nothing.
+std::shared_ptr<Plan> get_plan_variant(int64_t d1, int64_t d2, int64_t d3, int eb, int kind, int64_t t,
+                                       const Variant &v, int *status);
 // Whether get_plan would find this exact key in the cache (nothing is built).
 bool plan_cached(int64_t d1, int64_t d2, int64_t d3, int eb, int kind, int64_t t);
 // Runs a plan on `data` (d1*d2*d3*eb bytes) on stream st.

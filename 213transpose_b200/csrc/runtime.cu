@@ -600,8 +600,9 @@ struct PlanKey {
   int eb, kind;
   int64_t t;
   int dev;
+  int var = 0;  // Variant::packed()
   bool operator<(const PlanKey &o) const {
-    return std::tie(d1, d2, d3, eb, kind, t, dev) < std::tie(o.d1, o.d2, o.d3, o.eb, o.kind, o.t, o.dev);
+    return std::tie(d1, d2, d3, eb, kind, t, dev, var) < std::tie(o.d1, o.d2, o.d3, o.eb, o.kind, o.t, o.dev, o.var);
   }
 };
 
@@ -627,7 +628,32 @@ std::shared_ptr<Plan> new_plan(int64_t d1, int64_t d2, int64_t d3, int eb) {
 
 }  // namespace
 
-int tuner_lookup_internal(int64_t d1, int64_t d2, int64_t d3, int eb, int *kind, int64_t *t);
+int tuner_lookup_internal(int64_t d1, int64_t d2, int64_t d3, int eb, int *kind, int64_t *t, Variant *v);
+
+std::shared_ptr<Plan> get_plan_variant(int64_t d1, int64_t d2, int64_t d3, int eb, int kind, int64_t t,
+                                       const Variant &v, int *status) {
+  std::shared_ptr<Plan> base = get_plan(d1, d2, d3, eb, kind, t, status);
+  if (!base || !v.any()) return base;
+  PlanKey key{d1, d2, d3, eb, kind, t, dev_info().id, v.packed()};
+  std::lock_guard<std::mutex> lk(g_plan_mu);
+  auto it = g_plans.find(key);
+  if (it != g_plans.end()) {
+    g_plan_lru.splice(g_plan_lru.begin(), g_plan_lru, it->second);
+    return it->second->second;
+  }
+  auto P = std::make_shared<Plan>(*base);
+  P->var = v;
+  char buf[64];
+  snprintf(buf, sizeof buf, " [variant col=%d row=%d tile=%d seg=%d]", v.col, v.row, v.tile, v.seg);
+  P->desc += buf;
+  g_plan_lru.emplace_front(key, P);
+  g_plans[key] = g_plan_lru.begin();
+  while (g_plan_lru.size() > kPlanCacheMax) {
+    g_plans.erase(g_plan_lru.back().first);
+    g_plan_lru.pop_back();
+  }
+  return P;
+}
 
 bool plan_cached(int64_t d1, int64_t d2, int64_t d3, int eb, int kind, int64_t t) {
   PlanKey key{d1, d2, d3, eb, kind, t, dev_info().id};
@@ -641,9 +667,12 @@ std::shared_ptr<Plan> get_plan(int64_t d1, int64_t d2, int64_t d3, int eb, int k
   if (kind == T213_PLAN_AUTO) {
     int tk = 0;
     int64_t tt = 0;
-    if (tuner_lookup_internal(d1, d2, d3, eb, &tk, &tt) == T213_OK && tk != T213_PLAN_AUTO) {
-      auto p = get_plan(d1, d2, d3, eb, tk, tt, status);
+    Variant tv;
+    if (tuner_lookup_internal(d1, d2, d3, eb, &tk, &tt, &tv) == T213_OK && tk != T213_PLAN_AUTO) {
+      auto p = get_plan_variant(d1, d2, d3, eb, tk, tt, tv, status);
+      if (!p && tt) p = get_plan_variant(d1, d2, d3, eb, tk, 0, tv, status);  // block size of another shape
       if (p) return p;
+      *status = T213_OK;
     }
   }
   PlanKey key{d1, d2, d3, eb, kind, t, dev};
@@ -756,8 +785,17 @@ size_t plan_workspace_bytes(const Plan &p) {
   return w;
 }
 
+namespace {
+thread_local Variant t_variant;
+}  // namespace
+
+const Variant &current_variant() { return t_variant; }
+VariantScope::VariantScope(const Variant &v) : saved(t_variant) { t_variant = v; }
+VariantScope::~VariantScope() { t_variant = saved; }
+
 int run_plan(const Plan &P, char *data, cudaStream_t st, LaunchStats *ls) {
   const int64_t slice_bytes = P.d1 * P.d2 * P.eb;
+  VariantScope vs(P.var);
   for (const PassDesc &p : P.passes) {
     PassTimer tm(p.name(), st);
     int rc = T213_OK;
