@@ -793,30 +793,49 @@ const Variant &current_variant() { return t_variant; }
 VariantScope::VariantScope(const Variant &v) : saved(t_variant) { t_variant = v; }
 VariantScope::~VariantScope() { t_variant = saved; }
 
+// Slices per group when a plan runs its passes group by group
+// (T213_SLICE_GROUP_MB: the group's size in MB; unset or 0: all slices in
+// one group).  Every pass of a group runs before the next group starts, so a
+// pass finds part of what the previous pass wrote still in L2.
+int64_t slice_group(const Plan &P) {
+  static const int64_t mb = [] {
+    const char *v = std::getenv("T213_SLICE_GROUP_MB");
+    return v ? (int64_t)std::atoll(v) : 0;
+  }();
+  const int64_t slice_bytes = P.d1 * P.d2 * P.eb;
+  if (mb <= 0 || slice_bytes <= 0 || P.d3 <= 1) return std::max<int64_t>(1, P.d3);
+  return std::max<int64_t>(1, std::min<int64_t>(P.d3, (mb << 20) / slice_bytes));
+}
+
 int run_plan(const Plan &P, char *data, cudaStream_t st, LaunchStats *ls) {
   const int64_t slice_bytes = P.d1 * P.d2 * P.eb;
   VariantScope vs(P.var);
-  for (const PassDesc &p : P.passes) {
-    PassTimer tm(p.name(), st);
-    int rc = T213_OK;
-    switch (p.type) {
-      case PT_COL:
-        rc = launch_col_gather(p.fn, data, P.d3, p.m, p.n, P.eb, st, ls);
-        break;
-      case PT_ROW:
-        rc = launch_row_gather(p.fn, data, P.d3, p.m, p.n, P.eb, st, ls);
-        break;
-      case PT_TILE:
-        rc = launch_tile_swap(data, P.d3, p.m, p.n, p.t, P.eb, st, ls);
-        break;
-      case PT_BAND:
-        rc = launch_band_transpose(data, P.d3 * p.bands, p.R, p.C, P.eb, st, ls);
-        break;
-      case PT_SEG:
-        rc = launch_seg_cycles(*p.table, data, P.d3, slice_bytes, p.seg_bytes, st, ls, nullptr, 0);
-        break;
+  const int64_t group = slice_group(P);
+  for (int64_t k0 = 0; k0 < P.d3; k0 += group) {
+    const int64_t g = std::min<int64_t>(group, P.d3 - k0);
+    char *gd = data + k0 * slice_bytes;
+    for (const PassDesc &p : P.passes) {
+      PassTimer tm(p.name(), st);
+      int rc = T213_OK;
+      switch (p.type) {
+        case PT_COL:
+          rc = launch_col_gather(p.fn, gd, g, p.m, p.n, P.eb, st, ls);
+          break;
+        case PT_ROW:
+          rc = launch_row_gather(p.fn, gd, g, p.m, p.n, P.eb, st, ls);
+          break;
+        case PT_TILE:
+          rc = launch_tile_swap(gd, g, p.m, p.n, p.t, P.eb, st, ls);
+          break;
+        case PT_BAND:
+          rc = launch_band_transpose(gd, g * p.bands, p.R, p.C, P.eb, st, ls);
+          break;
+        case PT_SEG:
+          rc = launch_seg_cycles(*p.table, gd, g, slice_bytes, p.seg_bytes, st, ls, nullptr, 0);
+          break;
+      }
+      if (rc) return rc;
     }
-    if (rc) return rc;
   }
   return T213_OK;
 }
@@ -1192,19 +1211,23 @@ int t213_plan_launches(int64_t d1, int64_t d2, int64_t d3, int32_t elem_bytes, i
   std::shared_ptr<Plan> P = get_plan(d1, d2, d3, elem_bytes, plan_kind, t, &rc);
   if (!P) return rc;
   int n = 0;
-  for (const PassDesc &p : P->passes) {
-    switch (p.type) {
-      case PT_COL:
-        n += count_col_gather(d3, p.m, p.n, elem_bytes);
-        break;
-      case PT_ROW:
-        n += count_row_gather(d3, p.m, p.n, elem_bytes);
-        break;
-      case PT_SEG:
-        n += (p.table->n_chunks > 0) + (p.table->n_carry > 0);
-        break;
-      default:
-        n += 1;
+  const int64_t group = slice_group(*P);
+  for (int64_t k0 = 0; k0 < d3; k0 += group) {
+    const int64_t g = std::min<int64_t>(group, d3 - k0);
+    for (const PassDesc &p : P->passes) {
+      switch (p.type) {
+        case PT_COL:
+          n += count_col_gather(g, p.m, p.n, elem_bytes);
+          break;
+        case PT_ROW:
+          n += count_row_gather(g, p.m, p.n, elem_bytes);
+          break;
+        case PT_SEG:
+          n += (p.table->n_chunks > 0) + (p.table->n_carry > 0);
+          break;
+        default:
+          n += 1;
+      }
     }
   }
   *launches = n;
