@@ -17,8 +17,15 @@ oracle/Makefile into oracle/_ref/libref_inplace.so) runs in a child process
   (1) c2r::col_op passes d2/c where fused_postop needs c (src/transpose.cu:22):
   fp32 (512, 384, 16), the first configuration, and (2^20, 48, 1).  (2) The
   8-byte register row shuffles launch without a slice offset
-  (src/shuffle.cu:40-49): fp64 (7919, 6151, 2), and the R2C form int64
-  (300, 7000, 2).
+  (src/shuffle.cu:40-49): fp64 (6500, 6151, 2), and the R2C form int64
+  (300, 6500, 2), both on the R = 18 variant (rows of 6144 to 6917
+  elements).
+* A shape the reference cannot run on sm_100a: rows of 6918 to 29695 8-byte
+  elements take register_row_shuffle<T, F, 57> with 512 threads
+  (src/shuffle.cu:44-48), which needs more registers than an SM has for that
+  block, so the launch is refused (cudaErrorLaunchOutOfResources) and the
+  reference's error check ends its process.  This is fp64 (7919, 6151, 2),
+  the coprime large configuration.  The refusal is host-side; nothing runs.
 
 Shapes are chosen so that the reference stays in bounds and its barriers stay
 uniform: every dimension that a column kernel strides over in 32-wide groups
@@ -71,9 +78,12 @@ SWEEP = _sweep()
 DIVERGENT = [
     ("fp32_512x384x16", 512, 384, 16, "float32", "uniform", 0, "postop", 3_121_152),
     ("fp32_2p20x48x1", 1 << 20, 48, 1, "float32", "bits", 5, "postop", None),
-    ("fp64_7919x6151x2", 7919, 6151, 2, "float64", "uniform", 0, "reg8", None),
-    ("int64_300x7000x2", 300, 7000, 2, "int64", "bits", 6, "reg8", None),
+    ("fp64_6500x6151x2", 6500, 6151, 2, "float64", "uniform", 0, "reg8", None),
+    ("int64_300x6500x2", 300, 6500, 2, "int64", "bits", 6, "reg8", None),
 ]
+
+# shapes whose reference launch is refused on sm_100a (each in a child of its own)
+REFUSED = [("fp64_7919x6151x2", 7919, 6151, 2, "float64", "uniform", 0)]
 
 SAVE_LIMIT = 64 << 20  # results up to this size come back as bytes
 
@@ -141,6 +151,22 @@ def test_reference_gpu_sweep(ref_results, cuda, oracle, t213, case):
     assert np.array_equal(got, want), "ours differs from the gather oracle"
     if np.array_equal(emulated, want):
         assert np.array_equal(r["bytes"], got), "the reference's GPU output differs from ours"
+
+
+@pytest.mark.parametrize("case", REFUSED, ids=[c[0] for c in REFUSED])
+def test_reference_gpu_launch_refused_on_sm100(cuda, oracle, t213, tmp_path, case):
+    name, d1, d2, d3, typ, gen, seed = case
+    eb = _eb(typ)
+    jf, rf = tmp_path / "jobs.json", tmp_path / "results.json"
+    jf.write_text(json.dumps([{"name": name, "d1": d1, "d2": d2, "d3": d3, "type": typ, "gen": gen, "seed": seed}]))
+    r = subprocess.run([sys.executable, os.path.join(HERE, "ref_gpu_child.py"), str(jf), str(rf)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode != 0
+    assert "register 58 shuffle" in r.stderr and "too many resources requested for launch" in r.stderr, r.stderr
+    # ours transposes it exactly
+    x = child.make_input(gen, d1 * d2 * d3, eb, seed)
+    want = oracle.gather213(x.view(np.dtype((np.void, eb))), d1, d2, d3).view(np.uint8)
+    assert np.array_equal(_ours(cuda, t213, x, d1, d2, d3, eb), want)
 
 
 @pytest.mark.parametrize("case", DIVERGENT, ids=[c[0] for c in DIVERGENT])
