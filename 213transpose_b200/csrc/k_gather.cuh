@@ -515,6 +515,206 @@ __global__ void __launch_bounds__(kGatherThreads)
   }
 }
 
+// Double-buffered form of k_col_local: shared memory holds two strips, and
+// the loads of a CTA's next strip are issued right after the barrier that
+// ends the current strip's loads, so they are in flight while the current
+// strip is written back.  One cluster (or CTA) barrier per strip orders (a)
+// every load of strip u before any store of strip u, and (b) every store of
+// the strip before u (which read the other buffer) before that buffer is
+// loaded again.  Strips of one CTA are different columns, so the next strip's
+// loads never read what the current strip's stores write.
+template <int EB, int AW, typename U, typename Off, typename Fsrc, typename Gout, bool CLUSTER>
+__global__ void __launch_bounds__(kGatherThreads)
+    k_col_local_db(char *__restrict__ data, int64_t d3, U m, U n, U W, U WS, int64_t n_strips, U H, int halo,
+                   Off off, Fsrc F, Gout G, int64_t buf_elems, int *status) {
+  using E = typename ElemT<EB>::type;
+  using Wd = typename WordT<AW>::type;
+  using P = Pack<AW, EB>;
+  constexpr int PER = AW / EB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int s_sh[2][256];
+  __shared__ int s_span[2];
+  __shared__ U s_base[2];
+
+  int rank = 0, K = 1;
+  int64_t unit0 = blockIdx.x, ustride = gridDim.x;
+  if (CLUSTER) {
+    cg::cluster_group cl = cg::this_cluster();
+    rank = (int)cl.block_rank();
+    K = (int)cl.num_blocks();
+    unit0 = blockIdx.x / K;
+    ustride = gridDim.x / K;
+  }
+  const bool whole = !CLUSTER && H >= m;
+  const int64_t n_units = d3 * n_strips;
+  const U k0 = (U)min((int64_t)rank * (int64_t)H, (int64_t)m);
+  const U k1 = (U)min((int64_t)k0 + (int64_t)H, (int64_t)m);
+  const U nk = k1 - k0;
+  const int64_t pitch = (int64_t)n * EB;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+
+  struct Geo {
+    char *sbase;
+    U j0, wn;
+    uint32_t wpr;
+  };
+  auto geo = [&](int64_t u) {
+    Geo g;
+    const int64_t k = u / n_strips;
+    const U s = (U)(u - k * n_strips);
+    g.j0 = s * W;
+    g.wn = min(W, n - g.j0);  // multiple of PER
+    g.wpr = (uint32_t)(g.wn / PER);
+    g.sbase = data + (k * (int64_t)m * n + g.j0) * EB;
+    return g;
+  };
+  // warp 0: the strip's column offsets into slot b
+  auto prep = [&](const Geo &g, int b) {
+    const int64_t mm = (int64_t)m;
+    const int64_t r0 = (int64_t)off(g.j0);
+    int dmin = 0, dmax = 0;
+    for (U w = lane; w < g.wn; w += 32) {
+      const int64_t rw = (int64_t)off(g.j0 + w);
+      int64_t d = rw - r0;
+      if (2 * d > mm) d -= mm;
+      if (2 * d <= -mm) d += mm;
+      s_sh[b][w] = whole ? (int)rw : (int)d;
+      dmin = min(dmin, (int)d);
+      dmax = max(dmax, (int)d);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      dmin = min(dmin, __shfl_xor_sync(0xffffffffu, dmin, o));
+      dmax = max(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+    }
+    __syncwarp();
+    if (!whole)
+      for (U w = lane; w < g.wn; w += 32) s_sh[b][w] -= dmin;
+    if (lane == 0) {
+      s_span[b] = whole ? 0 : dmax - dmin;
+      int64_t bb = whole ? 0 : ((int64_t)k0 + r0 + dmin) % mm;
+      if (bb < 0) bb += mm;
+      s_base[b] = (U)bb;
+    }
+  };
+  auto key_of_slot = [&](U sl, U base) -> U {
+    U key = base + sl;
+    return key >= m ? key - m : key;
+  };
+  auto slot_of = [&](U o, int sh) -> U {
+    if (whole) {
+      U v = k0 + o + (U)sh;
+      return v >= m ? v - m : v;
+    }
+    return o + (U)sh;
+  };
+  // the host sized shared memory for its own scan of every strip's span; a
+  // strip that needs more records an error and moves no data
+  auto slots_of = [&](int b) -> U {
+    if (s_span[b] > halo) return 0;
+    return whole ? m : (nk > 0 ? nk + (U)s_span[b] : 0);
+  };
+  auto load = [&](const Geo &g, int b) {
+    E *sm = reinterpret_cast<E *>(smem_raw) + (int64_t)b * buf_elems;
+    const U nslots = slots_of(b);
+    const U base = s_base[b];
+    if (s_span[b] > halo && threadIdx.x == 0) atomicExch(status, 1 /* T213_ERR_INVALID_ARGUMENT */);
+    if (32 % g.wpr == 0) {
+      const uint32_t rpi = 32 / g.wpr, lr = lane / g.wpr, lw = lane - lr * g.wpr;
+      for (U sb = (U)warp * 32; sb < nslots; sb += (U)nwarps * 32) {
+        const U mys = sb + lane;
+        const U myrow = mys < nslots ? F(key_of_slot(mys, base)) : 0;
+        for (uint32_t r = lr; r < 32; r += rpi) {
+          const U row = __shfl_sync(0xffffffffu, myrow, r);
+          const U sl = sb + r;
+          if (sl < nslots) {
+            const Wd *gp = reinterpret_cast<const Wd *>(g.sbase + (int64_t)row * pitch) + lw;
+            Wd *dp = reinterpret_cast<Wd *>(sm + (int64_t)sl * WS) + lw;
+            if constexpr (AW >= 4)
+              cp_async<AW>(dp, gp);
+            else
+              *dp = __ldcs(gp);
+          }
+        }
+      }
+    } else {
+      const uint32_t nw = (uint32_t)nslots * g.wpr;
+      for (uint32_t t = threadIdx.x; t < nw; t += blockDim.x) {
+        const uint32_t sl = t / g.wpr, w = t - sl * g.wpr;
+        const U row = F(key_of_slot((U)sl, base));
+        const Wd *gp = reinterpret_cast<const Wd *>(g.sbase + (int64_t)row * pitch) + w;
+        if constexpr (AW >= 4)
+          cp_async<AW>(reinterpret_cast<Wd *>(sm + (int64_t)sl * WS) + w, gp);
+        else
+          reinterpret_cast<Wd *>(sm + (int64_t)sl * WS)[w] = __ldcs(gp);
+      }
+    }
+  };
+  auto store = [&](const Geo &g, int b) {
+    const E *sm = reinterpret_cast<const E *>(smem_raw) + (int64_t)b * buf_elems;
+    const U nout = s_span[b] <= halo ? nk : 0;
+    if (32 % g.wpr == 0) {
+      const uint32_t rpi = 32 / g.wpr, lr = lane / g.wpr, lw = lane - lr * g.wpr;
+      int sh[PER];
+#pragma unroll
+      for (int e = 0; e < PER; e++) sh[e] = s_sh[b][lw * PER + e];
+      for (U ob = (U)warp * 32; ob < nout; ob += (U)nwarps * 32) {
+        const U myo = ob + lane;
+        const U myrow = myo < nout ? G(k0 + myo) : 0;
+        for (uint32_t r = lr; r < 32; r += rpi) {
+          const U row = __shfl_sync(0xffffffffu, myrow, r);
+          const U o = ob + r;
+          if (o < nout) {
+            typename P::U pk;
+#pragma unroll
+            for (int e = 0; e < PER; e++) pk.e[e] = sm[(int64_t)slot_of(o, sh[e]) * WS + lw * PER + e];
+            __stcs(reinterpret_cast<Wd *>(g.sbase + (int64_t)row * pitch) + lw, pk.w);
+          }
+        }
+      }
+    } else {
+      const uint32_t nwo = (uint32_t)nout * g.wpr;
+      for (uint32_t t = threadIdx.x; t < nwo; t += blockDim.x) {
+        const uint32_t o = t / g.wpr, w = t - o * g.wpr;
+        const U row = G(k0 + (U)o);
+        typename P::U pk;
+#pragma unroll
+        for (int e = 0; e < PER; e++) {
+          const int c = (int)(w * PER + e);
+          pk.e[e] = sm[(int64_t)slot_of((U)o, s_sh[b][c]) * WS + c];
+        }
+        __stcs(reinterpret_cast<Wd *>(g.sbase + (int64_t)row * pitch) + w, pk.w);
+      }
+    }
+  };
+  auto barrier = [&]() {
+    if (CLUSTER)
+      cg::this_cluster().sync();
+    else
+      __syncthreads();
+  };
+
+  int64_t u = unit0;
+  if (u >= n_units) return;  // the same for every CTA of a cluster
+  Geo cur = geo(u);
+  if (warp == 0) prep(cur, 0);
+  __syncthreads();
+  load(cur, 0);
+  for (int b = 0; u < n_units; u += ustride, b ^= 1) {
+    if constexpr (AW >= 4) cp_async_wait_all();  // this strip's loads (the only ones in flight)
+    barrier();  // (a) strip u loaded everywhere; (b) the previous strip's stores are done
+    const int64_t un = u + ustride;
+    Geo nxt;
+    if (un < n_units) {
+      nxt = geo(un);
+      if (warp == 0) prep(nxt, b ^ 1);
+      __syncthreads();
+      load(nxt, b ^ 1);  // in flight during the stores below
+    }
+    store(cur, b);
+    cur = nxt;
+  }
+}
+
 // Column groups too tall for a cluster: the host copied columns
 // [j_lo, j_lo+gw) of every row of slice k to `scratch` (row pitch gw elements)
 // with one 2-D device-to-device copy; this kernel gathers from that copy.

@@ -177,8 +177,9 @@ int local_form(int kind) {
 struct LocalCfg {
   bool ok = false;
   int aw = 4, K = 1;
-  int64_t W = 0, WS = 0, H = 0, halo = 0, smem = 0;
+  int64_t W = 0, WS = 0, H = 0, halo = 0, smem = 0;  // smem: one strip buffer
   bool u64 = false;
+  bool db = false;  // double-buffered kernel (two strip buffers)
 };
 
 // Largest (dmax - dmin) over the strips of width W: the key offsets of one
@@ -277,7 +278,13 @@ LocalCfg local_col_config(const FnSpec &f, int64_t m, int64_t n, int eb, const v
   // index width: the functor's own bound, and the permutation maps' products
   // (below a * a with a = m / gcd)
   c.u64 = !fits32(f, m, n) || (double)m * (double)m >= 2.0e9;
-  const int64_t whole_cap = (env_int("T213_COL_WHOLE_KB") > 0 ? env_int("T213_COL_WHOLE_KB") : 104) * 1024;
+  // double-buffered kernel (T213_COL_DB or the pinned variant): 1 keeps the
+  // strip sizes below, 2 halves them (twice the cluster size) so two CTAs
+  // share an SM
+  const int dbmode = pv.col == 3 ? 1 : pv.col == 4 ? 2 : env_int("T213_COL_DB");
+  const int64_t buf_cap = dbmode ? kSmemCap / 2 - 64 : kSmemCap;
+  const int64_t whole_cap =
+      std::min<int64_t>(buf_cap, (env_int("T213_COL_WHOLE_KB") > 0 ? env_int("T213_COL_WHOLE_KB") : 104) * 1024);
   if (m * 128 <= whole_cap && env_int("T213_COL_LOCAL_K") <= 1 && pv.col != 2) {
     // whole strips in one CTA: at least 128-byte rows, widened to about
     // 48 KB per strip (at most 256 columns), no halo
@@ -289,6 +296,7 @@ LocalCfg local_col_config(const FnSpec &f, int64_t m, int64_t n, int eb, const v
     c.halo = 0;
     c.smem = m * c.WS * eb;
     c.ok = true;
+    c.db = dbmode != 0;
     return c;
   }
   // tall strips: 128-byte strips over a cluster of up to 16 CTAs of about
@@ -303,6 +311,10 @@ LocalCfg local_col_config(const FnSpec &f, int64_t m, int64_t n, int eb, const v
                      env_int("T213_COL_LOCAL_SMEM_KB") > 0 ? env_int("T213_COL_LOCAL_SMEM_KB") : 100});
   else if (pv.col == 2)  // 256-byte strips: longer DRAM bursts, fewer CTAs per SM
     tries = {{256, 110}, {256, 200}, {128, 100}, {128, 200}, {64, 200}, {32, 200}, {16, 200}};
+  else if (dbmode == 2)
+    tries = {{128, 50}, {128, 110}, {64, 110}, {32, 110}, {16, 110}};
+  else if (dbmode)
+    tries = {{128, 100}, {128, 110}, {64, 110}, {32, 110}, {16, 110}};
   else
     tries = {{128, 100}, {128, 200}, {64, 200}, {32, 200}, {16, 200}};
   for (const Try &t : tries) {
@@ -317,8 +329,9 @@ LocalCfg local_col_config(const FnSpec &f, int64_t m, int64_t n, int eb, const v
     if (c.K > kMaxCluster || c.K < 2) continue;
     c.H = (m + c.K - 1) / c.K;
     c.smem = (c.H + c.halo) * row_bytes;
-    if (c.smem > kSmemCap) continue;
+    if (c.smem > buf_cap) continue;
     c.ok = true;
+    c.db = dbmode != 0;
     return c;
   }
   return c;
@@ -468,8 +481,8 @@ std::string describe_col_gather_fn(const FnSpec &f, int64_t m, int64_t n, int eb
   LocalCfg lc = local_col_config(f, m, n, eb, data);
   if (lc.ok) {
     char buf[160];
-    snprintf(buf, sizeof buf, "col_gather[local W=%lld cluster=%d halo=%lld smem=%lldK aw=%d]", (long long)lc.W, lc.K,
-             (long long)lc.halo, (long long)(lc.smem / 1024), lc.aw);
+    snprintf(buf, sizeof buf, "col_gather[local%s W=%lld cluster=%d halo=%lld smem=%lldK aw=%d]", lc.db ? " db" : "",
+             (long long)lc.W, lc.K, (long long)lc.halo, (long long)((lc.db ? 2 : 1) * lc.smem / 1024), lc.aw);
     return buf;
   }
   return describe_col_gather(m, n, eb, data);
@@ -543,6 +556,28 @@ int launch_col_local_t(const FnSpec &f, const LocalCfg &c, char *data, int64_t d
     using Gs = decltype(G);
     int *stw = device_status_word(&status);
     if (!stw) return;
+    if (c.db) {
+      const int64_t buf_elems = (c.smem + 15) / 16 * 16 / EB;
+      const int64_t smem2 = 2 * buf_elems * EB;
+      if (c.K == 1) {
+        auto kern = k_col_local_db<EB, AW, U, Off, Fs, Gs, false>;
+        if ((status = prep_kernel(kern, smem2, 1))) return;
+        const int64_t grid = persistent_grid(kern, kGatherThreads, smem2, 1, units);
+        status = launch_k(kern, grid, kGatherThreads, smem2, 1, st, data, d3, (U)m, (U)n, (U)c.W, (U)c.WS, n_strips,
+                          (U)c.H, (int)c.halo, off, F, G, buf_elems, stw);
+      } else {
+        auto kern = k_col_local_db<EB, AW, U, Off, Fs, Gs, true>;
+        if ((status = prep_kernel(kern, smem2, c.K))) return;
+        if (clusters_resident((const void *)kern, kGatherThreads, smem2, c.K) < 1) {
+          status = kNoCluster;
+          return;
+        }
+        const int64_t grid = persistent_grid(kern, kGatherThreads, smem2, c.K, units);
+        status = launch_k(kern, grid, kGatherThreads, smem2, c.K, st, data, d3, (U)m, (U)n, (U)c.W, (U)c.WS,
+                          n_strips, (U)c.H, (int)c.halo, off, F, G, buf_elems, stw);
+      }
+      return;
+    }
     if (c.K == 1) {
       auto kern = k_col_local<EB, AW, U, Off, Fs, Gs, false>;
       if ((status = prep_kernel(kern, c.smem, 1))) return;

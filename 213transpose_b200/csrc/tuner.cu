@@ -1,7 +1,7 @@
 // Autotuner: times the applicable plan families of a shape on the device,
 // then, for the winning family, its block or band size and the kernel
-// variants of its passes (column strips staged or cluster-local and their
-// width, staged or double-buffered rows, TMA or register tile swaps, bulk
+// variants of its passes (column strips staged or cluster-local, their width,
+// single- or double-buffered, staged or double-buffered rows, TMA or register tile swaps, bulk
 // walker ring depth or the register walker), one choice at a time, and caches
 // the winner per exact shape and per shape class.  A class is (element size,
 // log2 of d1, d2 and d3, log2 of gcd(d1,d2)); a class entry keeps the family
@@ -210,7 +210,7 @@ int t213_tune_shape(void *scratch_data, int64_t d1, int64_t d2, int64_t d3, int3
       int8_t Variant::*field;
       std::vector<int8_t> values;
     };
-    const Knob knobs[] = {{PT_COL, &Variant::col, {1, 2}},
+    const Knob knobs[] = {{PT_COL, &Variant::col, {1, 2, 3, 4}},
                           {PT_ROW, &Variant::row, {2}},
                           {PT_TILE, &Variant::tile, {1, 2}},
                           {PT_SEG, &Variant::seg, {2, 3}}};

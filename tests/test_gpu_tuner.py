@@ -61,6 +61,11 @@ VARIANTS = [
     ((7919, 601, 1, 8), "c2r", 0, _var(col=1)),
     ((7919, 601, 1, 8), "c2r", 0, _var(col=2)),
     ((7919, 601, 1, 8), "c2r", 0, _var(row=2)),
+    ((7919, 601, 1, 8), "c2r", 0, _var(col=3)),
+    ((7919, 6151, 1, 8), "c2r", 0, _var(col=3)),
+    ((7919, 6151, 1, 8), "c2r", 0, _var(col=4)),
+    ((3001, 2000, 2, 4), "r2c", 0, _var(col=4)),
+    ((30, 100000, 1, 4), "skinny", 0, _var(col=3)),
     ((3001, 2000, 2, 4), "r2c", 0, _var(col=2, row=2)),
     ((3001, 2000, 2, 4), "r2c", 0, _var(col=1, row=1)),
     ((1024, 768, 2, 4), "blocks", 256, _var(tile=1)),
