@@ -25,8 +25,9 @@ ERR_BUDGET = 6
 ERR_NOT_READY = 7
 
 # plan families
-PLAN_AUTO, PLAN_C2R, PLAN_R2C, PLAN_SKINNY, PLAN_BLOCKS, PLAN_BANDS, PLAN_BANDS_T, PLAN_IDENTITY = range(8)
-PLAN_NAMES = {"auto": 0, "c2r": 1, "r2c": 2, "skinny": 3, "blocks": 4, "bands": 5, "bands_t": 6, "identity": 7}
+PLAN_AUTO, PLAN_C2R, PLAN_R2C, PLAN_SKINNY, PLAN_BLOCKS, PLAN_BANDS, PLAN_BANDS_T, PLAN_IDENTITY, PLAN_SLICE = range(9)
+PLAN_NAMES = {"auto": 0, "c2r": 1, "r2c": 2, "skinny": 3, "blocks": 4, "bands": 5, "bands_t": 6, "identity": 7,
+              "slice": 8}
 
 
 class T213Error(RuntimeError):

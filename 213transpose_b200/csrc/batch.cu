@@ -171,6 +171,8 @@ bool plan_fits_batch(const Plan &p) {
       case PT_BAND:
         if (q.R * q.C * p.eb > kBatchHalf) return false;
         break;
+      case PT_SLICE:  // a cluster launch of its own; no executor in the persistent kernel
+        return false;
       default:
         break;
     }

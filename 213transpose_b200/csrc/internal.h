@@ -153,6 +153,10 @@ int launch_tile_swap(char *data, int64_t d3, int64_t m, int64_t n, int64_t t, in
 int launch_band_transpose(char *data, int64_t n_bands, int64_t R, int64_t C, int eb, cudaStream_t st,
                           LaunchStats *ls);
 int64_t band_smem_bytes(int64_t R, int64_t C, int eb);
+// One-pass transpose of slices held whole in a cluster's shared memory.
+int launch_slice(char *data, int64_t d3, int64_t m, int64_t n, int eb, cudaStream_t st, LaunchStats *ls);
+bool slice_fits(int64_t m, int64_t n, int eb);
+std::string describe_slice(int64_t m, int64_t n, int eb, int64_t d3);
 int64_t band_smem_limit();
 bool band_fits(int64_t R, int64_t C, int eb);
 

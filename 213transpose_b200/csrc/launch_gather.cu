@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "k_gather.cuh"
+#include "k_slice.cuh"
 #include "plan.h"
 
 namespace t213 {
@@ -815,6 +816,109 @@ int launch_row_gather(const FnSpec &f, char *data, int64_t d3, int64_t m, int64_
   if (!known) {
     set_error("functor kind is not a row shuffle");
     return T213_ERR_INVALID_ARGUMENT;
+  }
+  return status;
+}
+
+
+// ------------------------------------------------------------------- slice --
+namespace {
+
+constexpr int64_t kSliceSmemCap = 220 * 1024;
+
+struct SliceCfg {
+  int K = 0;
+  uint32_t H = 0, P = 0;
+  int64_t smem = 0;
+  bool vec = false;
+};
+
+// Cluster size, rows per CTA and padded row pitch for one-pass slices; K = 0
+// when the slice does not fit 16 CTAs.  The smallest cluster that holds the
+// slice, doubled (up to 8) while the slices still leave SMs idle.
+SliceCfg slice_config(int64_t m, int64_t n, int eb, int64_t d3, const void *data) {
+  SliceCfg c;
+  if (m < 2 || n < 2 || m > (1 << 24) || n > (1 << 24)) return c;
+  int64_t P = (n * eb + 15) / 16 * 16;
+  if ((P / 16) % 2 == 0) P += 16;  // consecutive rows in different 16-byte bank groups
+  auto rows = [&](int K) -> int64_t {
+    if (K == 1) return m;
+    return ((m + K - 1) / K + 31) / 32 * 32;
+  };
+  int K = 0;
+  for (int k : {1, 2, 4, 8, 16})
+    if (rows(k) * P <= kSliceSmemCap) {
+      K = k;
+      break;
+    }
+  if (!K) return c;
+  const int sms = dev_info().sms;
+  while (K < 8 && d3 * 2 * K <= sms && m / (2 * K) >= 32) K *= 2;
+  c.K = K;
+  c.H = (uint32_t)rows(K);
+  c.P = (uint32_t)P;
+  c.smem = (int64_t)c.H * P;
+  c.vec = (n * eb) % 16 == 0 && (m * eb) % 16 == 0 && ((uintptr_t)data % 16) == 0;
+  return c;
+}
+
+}  // namespace
+
+bool slice_fits(int64_t m, int64_t n, int eb) { return slice_config(m, n, eb, 1, nullptr).K > 0; }
+
+std::string describe_slice(int64_t m, int64_t n, int eb, int64_t d3) {
+  SliceCfg c = slice_config(m, n, eb, d3, nullptr);
+  char buf[96];
+  snprintf(buf, sizeof buf, "slice(cluster=%d rows/cta=%u smem=%lldK)", c.K, c.H, (long long)(c.smem / 1024));
+  return buf;
+}
+
+int launch_slice(char *data, int64_t d3, int64_t m, int64_t n, int eb, cudaStream_t st, LaunchStats *ls) {
+  if (d3 <= 0 || m <= 0 || n <= 0) return T213_OK;
+  const SliceCfg c = slice_config(m, n, eb, d3, data);
+  if (!c.K) {
+    set_error("slice does not fit a cluster's shared memory");
+    return T213_ERR_UNSUPPORTED;
+  }
+  int status = T213_ERR_UNSUPPORTED;
+  auto go = [&](auto kern) {
+    if ((status = prep_kernel(kern, c.smem, c.K))) return;
+    int64_t clusters = d3;
+    if (c.K > 1) {
+      const int res = clusters_resident((const void *)kern, kSliceThreads, c.smem, c.K);
+      if (res < 1) {
+        status = cuda_status(cudaErrorInvalidConfiguration, "slice cluster cannot be resident");
+        return;
+      }
+      clusters = std::min<int64_t>(d3, res);
+    } else {
+      int per_sm = 1;
+      occupancy_cached((const void *)kern, kSliceThreads, c.smem, 1, &per_sm);
+      clusters = std::min<int64_t>(d3, (int64_t)std::max(1, per_sm) * dev_info().sms);
+    }
+    status = launch_k(kern, clusters * c.K, kSliceThreads, c.smem, c.K, st, data, d3, (uint32_t)m, (uint32_t)n, c.H,
+                      c.P);
+    if (ls) ls->launches++;
+  };
+  auto pick = [&](auto EBc) {
+    constexpr int EB = decltype(EBc)::value;
+    if (c.vec) {
+      if (c.K > 1) go(k_slice<EB, true, true>);
+      else go(k_slice<EB, true, false>);
+    } else {
+      if (c.K > 1) go(k_slice<EB, false, true>);
+      else go(k_slice<EB, false, false>);
+    }
+  };
+  switch (eb) {
+    case 1: pick(IC<1>{}); break;
+    case 2: pick(IC<2>{}); break;
+    case 4: pick(IC<4>{}); break;
+    case 8: pick(IC<8>{}); break;
+    case 16: pick(IC<16>{}); break;
+    default:
+      set_error("unsupported element size");
+      return T213_ERR_UNSUPPORTED;
   }
   return status;
 }

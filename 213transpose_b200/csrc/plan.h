@@ -9,7 +9,7 @@
 
 namespace t213 {
 
-enum PassType { PT_COL = 1, PT_ROW = 2, PT_SEG = 3, PT_TILE = 4, PT_BAND = 5 };
+enum PassType { PT_COL = 1, PT_ROW = 2, PT_SEG = 3, PT_TILE = 4, PT_BAND = 5, PT_SLICE = 6 };
 
 struct PassDesc {
   PassType type = PT_COL;

@@ -252,6 +252,8 @@ const char *PassDesc::name() const {
       return "tile_swap";
     case PT_BAND:
       return "band_transpose";
+    case PT_SLICE:
+      return "slice";
   }
   return "?";
 }
@@ -309,8 +311,8 @@ double seg_eff(int64_t seg_bytes) {
 }
 
 std::string fmt_plan(const Plan &P) {
-  static const char *kn[] = {"auto", "c2r", "r2c", "skinny", "blocks", "bands", "bands_t", "identity"};
-  std::string s = kn[P.kind >= 0 && P.kind <= 7 ? P.kind : 0];
+  static const char *kn[] = {"auto", "c2r", "r2c", "skinny", "blocks", "bands", "bands_t", "identity", "slice"};
+  std::string s = kn[P.kind >= 0 && P.kind <= 8 ? P.kind : 0];
   char buf[256];
   if (P.t) {
     snprintf(buf, sizeof buf, " t=%lld", (long long)P.t);
@@ -329,6 +331,9 @@ std::string fmt_plan(const Plan &P) {
         break;
       case PT_ROW:
         snprintf(buf, sizeof buf, "row_gather(fn=%d)%s", p.fn.kind, describe_row_gather(p.m, p.n, P.eb, nullptr).substr(10).c_str());
+        break;
+      case PT_SLICE:
+        snprintf(buf, sizeof buf, "%s", describe_slice(p.m, p.n, P.eb, P.d3).c_str());
         break;
       case PT_SEG:
         snprintf(buf, sizeof buf, "segment_cycles(S=%lld seg=%lldB cycles=%lld chunks=%lld carry=%lld maxlen=%lld)",
@@ -519,6 +524,18 @@ int build_plan(Plan &P, int kind, int64_t t) {
       ps.S = (m / t) * n;
       return add_seg_pass(P, ps, t * eb, true);
     }
+    case T213_PLAN_SLICE: {
+      if (!slice_fits(m, n, eb)) {
+        set_error("slice plan needs a slice that fits a 16-CTA cluster's shared memory");
+        return T213_ERR_UNSUPPORTED;
+      }
+      PassDesc sp;
+      sp.type = PT_SLICE;
+      sp.m = m;
+      sp.n = n;
+      P.passes.push_back(sp);
+      return T213_OK;
+    }
     case T213_PLAN_BANDS_T: {
       if (t <= 0) t = pick_band_t_t(m, n, eb);
       if (t <= 0 || n % t || !band_fits(m, t, eb)) {
@@ -564,6 +581,9 @@ double plan_cost(const Plan &P) {
         break;
       case PT_BAND:
         c += 1 / 0.5;
+        break;
+      case PT_SLICE:
+        c += 1 / 0.6;
         break;
     }
   }
@@ -712,6 +732,8 @@ std::shared_ptr<Plan> get_plan(int64_t d1, int64_t d2, int64_t d3, int eb, int k
       cands.push_back({T213_PLAN_BANDS, tr, estimate_cost(T213_PLAN_BANDS, m, n, tr, eb, d3)});
       int64_t tc = pick_band_t_t(m, n, eb);
       cands.push_back({T213_PLAN_BANDS_T, tc, estimate_cost(T213_PLAN_BANDS_T, m, n, tc, eb, d3)});
+      // one pass through a cluster's shared memory for slices of a few MB
+      if (slice_fits(m, n, eb)) cands.push_back({T213_PLAN_SLICE, 0, 1 / 0.6});
       // The Catanzaro decomposition both ways: the reference's dispatcher
       // takes C2R when d1 >= d2, else R2C (src/transpose.cu:117-123); here
       // both are costed, since which one keeps its rows inside shared
@@ -832,6 +854,9 @@ int run_plan(const Plan &P, char *data, cudaStream_t st, LaunchStats *ls) {
           break;
         case PT_SEG:
           rc = launch_seg_cycles(*p.table, gd, g, slice_bytes, p.seg_bytes, st, ls, nullptr, 0);
+          break;
+        case PT_SLICE:
+          rc = launch_slice(gd, g, p.m, p.n, P.eb, st, ls);
           break;
       }
       if (rc) return rc;
@@ -1058,7 +1083,7 @@ int t213_transpose(void *data, int64_t d1, int64_t d2, int64_t d3, int32_t elem_
 
 int t213_transpose_with_plan(void *data, int64_t d1, int64_t d2, int64_t d3, int32_t elem_bytes, int32_t plan_kind,
                              int64_t t, t213_stream_t stream) {
-  if (plan_kind < T213_PLAN_AUTO || plan_kind > T213_PLAN_IDENTITY || t < 0) {
+  if (plan_kind < T213_PLAN_AUTO || plan_kind > T213_PLAN_SLICE || t < 0) {
     set_error("bad plan kind or block size");
     return T213_ERR_INVALID_ARGUMENT;
   }

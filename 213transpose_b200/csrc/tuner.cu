@@ -125,13 +125,13 @@ int t213_tuner_load(const char *path) {
     long long a, b, c, t = 0;
     // older files have no variant (and no block size on shape lines)
     const int nc = sscanf(line, "class %d %d %d %d %d %d %d", &k.eb, &k.l1, &k.l2, &k.l3, &k.lg, &kind, &var);
-    if (nc >= 6 && kind >= T213_PLAN_AUTO && kind <= T213_PLAN_IDENTITY) {
+    if (nc >= 6 && kind >= T213_PLAN_AUTO && kind <= T213_PLAN_SLICE) {
       g_cache[k] = Entry{kind, 0, nc == 7 ? var : 0};
       continue;
     }
     var = 0;
     const int ns = sscanf(line, "shape %lld %lld %lld %d %d %lld %d", &a, &b, &c, &eb, &kind, &t, &var);
-    if (ns >= 5 && kind >= T213_PLAN_AUTO && kind <= T213_PLAN_IDENTITY)
+    if (ns >= 5 && kind >= T213_PLAN_AUTO && kind <= T213_PLAN_SLICE)
       g_exact[std::make_tuple((int64_t)a, (int64_t)b, (int64_t)c, eb)] =
           Entry{kind, ns >= 6 ? (int64_t)t : 0, ns == 7 ? var : 0};
   }
@@ -171,7 +171,7 @@ int t213_tune_shape(void *scratch_data, int64_t d1, int64_t d2, int64_t d3, int3
   };
   // 1) the family, each with its planner-chosen block size and default kernels
   const int kinds[] = {T213_PLAN_BLOCKS, T213_PLAN_BANDS, T213_PLAN_BANDS_T, T213_PLAN_C2R, T213_PLAN_R2C,
-                       T213_PLAN_SKINNY};
+                       T213_PLAN_SKINNY, T213_PLAN_SLICE};
   double best_ms = 1e30;
   Entry best;
   for (int kind : kinds) {
@@ -202,7 +202,7 @@ int t213_tune_shape(void *scratch_data, int64_t d1, int64_t d2, int64_t d3, int3
   {
     int rc = T213_OK;
     std::shared_ptr<Plan> P = get_plan(d1, d2, d3, elem_bytes, best.kind, best.t, &rc);
-    bool has[6] = {false, false, false, false, false, false};
+    bool has[8] = {false, false, false, false, false, false, false, false};
     if (P)
       for (const PassDesc &q : P->passes) has[q.type] = true;
     struct Knob {

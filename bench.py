@@ -34,7 +34,7 @@ D1, D2, D3, EB = 8192, 6144, 4, 4
 D1B, D2B, D3B, EBB = 7919, 6151, 2, 8
 METRIC = "in-place 213 effective GB/s (2*bytes/time)"
 UNIT = "GB/s"
-PASSES = ("tile_swap", "segment_cycles", "row_gather", "col_gather", "band_transpose")
+PASSES = ("tile_swap", "segment_cycles", "row_gather", "col_gather", "band_transpose", "slice")
 FALLBACK_PEAK = 6650.0
 
 

@@ -78,7 +78,9 @@ typedef enum t213_plan_kind {
   T213_PLAN_BLOCKS = 4,    /* t x t square-block transposes + segment cycles (t | gcd)       */
   T213_PLAN_BANDS = 5,     /* band transposes + segment-matrix cycles (t | d2)              */
   T213_PLAN_BANDS_T = 6,   /* segment-matrix cycles + band transposes (t | d1)              */
-  T213_PLAN_IDENTITY = 7   /* d1 == 1 or d2 == 1: the memory layout does not change         */
+  T213_PLAN_IDENTITY = 7,  /* d1 == 1 or d2 == 1: the memory layout does not change         */
+  T213_PLAN_SLICE = 8      /* one pass: each slice held whole in a thread-block cluster's
+                              shared memory (slices up to a few MB)                         */
 } t213_plan_kind;
 
 const char *t213_status_string(int status);

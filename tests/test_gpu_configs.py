@@ -83,7 +83,7 @@ def test_config3_16byte_1024x1024(cuda, oracle, t213):
     _oracle_check(cuda, oracle, t213, x, d1, d2, d3, 16)
 
 
-@pytest.mark.parametrize("plan", ["c2r", "r2c", "skinny", "bands", "bands_t", "blocks"])
+@pytest.mark.parametrize("plan", ["c2r", "r2c", "skinny", "bands", "bands_t", "blocks", "slice"])
 def test_config3_skinny_every_applicable_plan(cuda, oracle, t213, plan):
     """Every decomposition that applies to a (mid-size) skinny shape agrees."""
     for d1, d2, d3, eb in [(32, 1 << 16, 2, 4), (1 << 16, 48, 1, 4), (3, 1 << 14, 4, 4)]:

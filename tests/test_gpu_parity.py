@@ -55,7 +55,7 @@ PLAN_SHAPES = [(64, 48, 2), (512, 384, 2), (100, 37, 1), (37, 100, 2), (600, 45,
 
 
 @pytest.mark.parametrize("eb", (4, 8, 16, 1))
-@pytest.mark.parametrize("plan", ["c2r", "r2c", "blocks", "bands", "bands_t", "skinny"])
+@pytest.mark.parametrize("plan", ["c2r", "r2c", "blocks", "bands", "bands_t", "skinny", "slice"])
 @pytest.mark.parametrize("shape", PLAN_SHAPES, ids=lambda s: "x".join(map(str, s)))
 def test_every_plan(cuda, oracle, t213, shape, plan, eb):
     d1, d2, d3 = shape

@@ -11,7 +11,7 @@ from conftest import from_device, to_device
 
 pytestmark = pytest.mark.gpu
 
-PLAN = {"c2r": 1, "r2c": 2, "skinny": 3, "blocks": 4, "bands": 5, "bands_t": 6}
+PLAN = {"c2r": 1, "r2c": 2, "skinny": 3, "blocks": 4, "bands": 5, "bands_t": 6, "slice": 8}
 
 
 def _var(col=0, row=0, tile=0, seg=0):
