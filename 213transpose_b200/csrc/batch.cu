@@ -365,13 +365,16 @@ std::shared_ptr<Plan> group_plan(int64_t d1, int64_t d2, int64_t d3, int eb, int
   std::shared_ptr<Plan> P = get_plan(d1, d2, d3, eb, T213_PLAN_AUTO, 0, status);
   if (!P) return nullptr;
   if (plan_fits_batch(*P)) return P;
-  // another family that fits the persistent kernel's shared memory
-  for (int k : {T213_PLAN_BLOCKS, T213_PLAN_BANDS, T213_PLAN_BANDS_T, T213_PLAN_C2R, T213_PLAN_R2C}) {
+  // the cheapest other family whose passes fit the persistent kernel's
+  // shared memory
+  std::shared_ptr<Plan> best;
+  for (int k : {T213_PLAN_BLOCKS, T213_PLAN_BANDS, T213_PLAN_BANDS_T, T213_PLAN_C2R, T213_PLAN_R2C,
+                T213_PLAN_SKINNY}) {
     int rc2 = T213_OK;
     auto Q = get_plan(d1, d2, d3, eb, k, 0, &rc2);
-    if (Q && plan_fits_batch(*Q)) return Q;
+    if (Q && plan_fits_batch(*Q) && (!best || Q->est_cost < best->est_cost)) best = Q;
   }
-  return nullptr;
+  return best;
 }
 
 struct GroupExec {

@@ -732,8 +732,10 @@ std::shared_ptr<Plan> get_plan(int64_t d1, int64_t d2, int64_t d3, int eb, int k
       cands.push_back({T213_PLAN_BANDS, tr, estimate_cost(T213_PLAN_BANDS, m, n, tr, eb, d3)});
       int64_t tc = pick_band_t_t(m, n, eb);
       cands.push_back({T213_PLAN_BANDS_T, tc, estimate_cost(T213_PLAN_BANDS_T, m, n, tc, eb, d3)});
-      // one pass through a cluster's shared memory for slices of a few MB
-      if (slice_fits(m, n, eb)) cands.push_back({T213_PLAN_SLICE, 0, 1 / 0.6});
+      // The one-pass cluster plan (T213_PLAN_SLICE) is not ranked here: on
+      // B200 it measured no faster than the two-sweep plans for slices of a
+      // few MB (the distributed shared-memory gathers are latency-bound), so
+      // it is taken only when forced or chosen by the tuner.
       // The Catanzaro decomposition both ways: the reference's dispatcher
       // takes C2R when d1 >= d2, else R2C (src/transpose.cu:117-123); here
       // both are costed, since which one keeps its rows inside shared
