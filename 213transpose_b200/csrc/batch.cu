@@ -10,6 +10,7 @@
 #include <tuple>
 
 #include "k_batch.cuh"
+#include "k_slice.cuh"
 #include "plan.h"
 
 using namespace t213;
@@ -45,6 +46,12 @@ struct t213_batch_st {
   // limit of every dependency wait of the persistent kernel (nanoseconds of
   // %globaltimer); lowered only by t213_batch_debug_stall
   uint64_t wait_ns = kWaitNs;
+  // small tensors transposed in one pass by a grouped cluster launch before
+  // the persistent kernel (their slices fit an 8-CTA cluster's shared memory)
+  std::vector<int> sliced;
+  SliceEntry *d_slices = nullptr;
+  int32_t n_slice_entries = 0;
+  int64_t n_slice_items = 0, slice_smem = 0;
 };
 
 namespace {
@@ -539,12 +546,47 @@ int t213_batch_create(const t213_tensor_desc *tensors, int32_t count, t213_batch
     B->plans.push_back(P);
   }
 
-  BatchTables T;
+  // ---- one-pass slices (T213_BATCH_SLICE=0 turns them off) -------------------
+  std::vector<char> skip(count, 0);
+  for (int i : B->spill) skip[i] = 1;
   {
-    std::vector<char> skip(count, 0);
-    for (int i : B->spill) skip[i] = 1;
-    if ((rc = build_batch_tables(tensors, count, B->plans, skip, T))) return fail(rc);
+    const char *sv = getenv("T213_BATCH_SLICE");
+    const bool on = !(sv && atoi(sv) == 0);
+    std::vector<SliceEntry> entries;
+    for (int32_t i = 0; i < count && on; i++) {
+      const t213_tensor_desc &d = tensors[i];
+      if (skip[i] || !B->plans[i] || d.plan_kind != T213_PLAN_AUTO || d.d1 * d.d2 * d.d3 == 0) continue;
+      uint32_t H = 0, P = 0;
+      bool vec = false;
+      // the element-wise form is kept for 8- and 16-byte elements, where it measured faster
+      if (!slice_group_params(d.d2, d.d1, d.elem_bytes, d.data, &H, &P, &vec) || !(vec || d.elem_bytes >= 8))
+        continue;
+      SliceEntry e{};
+      e.data = (char *)d.data;
+      e.d3 = d.d3;
+      e.first_item = B->n_slice_items;
+      e.m = (uint32_t)d.d2;
+      e.n = (uint32_t)d.d1;
+      e.H = H;
+      e.P = P;
+      e.eb = d.elem_bytes;
+      e.vec = vec ? 1 : 0;
+      entries.push_back(e);
+      B->n_slice_items += d.d3;
+      B->slice_smem = std::max<int64_t>(B->slice_smem, (int64_t)H * P);
+      B->sliced.push_back(i);
+      skip[i] = 1;
+    }
+    if (!entries.empty()) {
+      cudaError_t e = cudaMalloc(&B->d_slices, entries.size() * sizeof(SliceEntry));
+      if (e == cudaSuccess)
+        e = cudaMemcpy(B->d_slices, entries.data(), entries.size() * sizeof(SliceEntry), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) return fail(cuda_status(e, "batch slice entries"));
+      B->n_slice_entries = (int32_t)entries.size();
+    }
   }
+  BatchTables T;
+  if ((rc = build_batch_tables(tensors, count, B->plans, skip, T))) return fail(rc);
   B->h_passes = std::move(T.passes);
   B->h_items = std::move(T.items);
   // carry pool
@@ -608,10 +650,10 @@ int t213_batch_create(const t213_tensor_desc *tensors, int32_t count, t213_batch
   int64_t direct_bytes = 0;
   for (int i : B->spill) direct_bytes += tensors[i].d1 * tensors[i].d2 * tensors[i].d3 * tensors[i].elem_bytes;
   snprintf(buf, sizeof buf,
-           "batch: %d tensors, %.1f MB; persistent kernel: %d tensors, %zu passes, %zu items, grid %d x %d threads; "
-           "graph nodes: %d tensors, %.1f MB",
-           count, B->total_bytes / 1e6, count - (int)B->spill.size(), B->h_passes.size(), B->h_items.size(), B->grid,
-           kBatchThreads, (int)B->spill.size(), direct_bytes / 1e6);
+           "batch: %d tensors, %.1f MB; one-pass slices: %d tensors; persistent kernel: %d tensors, %zu passes, %zu "
+           "items, grid %d x %d threads; graph nodes: %d tensors, %.1f MB",
+           count, B->total_bytes / 1e6, (int)B->sliced.size(), count - (int)B->spill.size() - (int)B->sliced.size(),
+           B->h_passes.size(), B->h_items.size(), B->grid, kBatchThreads, (int)B->spill.size(), direct_bytes / 1e6);
   B->desc = buf;
   *out = B;
   return T213_OK;
@@ -625,6 +667,10 @@ static int batch_enqueue(t213_batch B, cudaStream_t st) {
   }
   e = cudaMemsetAsync(B->d_ctrs, 0, (B->n_ctrs + 1) * sizeof(unsigned long long), st);
   if (e != cudaSuccess) return cuda_status(e, "batch counters reset");
+  if (B->n_slice_entries > 0) {
+    int rc = launch_slice_group(B->d_slices, B->n_slice_entries, B->n_slice_items, B->slice_smem, st);
+    if (rc) return rc;
+  }
   if (!B->h_items.empty()) {
     k_batch<<<B->grid, kBatchThreads, (size_t)(kBatchSmem + kBatchBarBytes), st>>>(
         B->d_passes, B->d_items, (int64_t)B->h_items.size(), B->d_ctrs, B->d_ctrs + B->n_ctrs, B->d_status,
@@ -777,6 +823,7 @@ int t213_batch_destroy(t213_batch B) {
   if (B->d_ctrs) cudaFree(B->d_ctrs);
   if (B->d_status) cudaFree(B->d_status);
   if (B->d_carry) cudaFree(B->d_carry);
+  if (B->d_slices) cudaFree(B->d_slices);
   if (B->side) {
     release_stream_workspace(B->side);
     cudaStreamDestroy(B->side);

@@ -157,6 +157,11 @@ int64_t band_smem_bytes(int64_t R, int64_t C, int eb);
 int launch_slice(char *data, int64_t d3, int64_t m, int64_t n, int eb, cudaStream_t st, LaunchStats *ls);
 bool slice_fits(int64_t m, int64_t n, int eb);
 std::string describe_slice(int64_t m, int64_t n, int eb, int64_t d3);
+// Grouped one-pass slices (the batched form): the rows per CTA H and padded
+// pitch P of a slice split over an 8-CTA cluster (false if it does not fit),
+// and one launch of the grouped kernel over device SliceEntry records.
+bool slice_group_params(int64_t m, int64_t n, int eb, const void *data, uint32_t *H, uint32_t *P, bool *vec);
+int launch_slice_group(const void *entries, int32_t n_entries, int64_t n_items, int64_t smem, cudaStream_t st);
 int64_t band_smem_limit();
 bool band_fits(int64_t R, int64_t C, int eb);
 

@@ -825,6 +825,7 @@ int launch_row_gather(const FnSpec &f, char *data, int64_t d3, int64_t m, int64_
 namespace {
 
 constexpr int64_t kSliceSmemCap = 220 * 1024;
+constexpr int kSliceGroupK = 8;  // cluster size of the batched form's grouped slice launch
 
 struct SliceCfg {
   int K = 0;
@@ -865,6 +866,30 @@ SliceCfg slice_config(int64_t m, int64_t n, int eb, int64_t d3, const void *data
 }  // namespace
 
 bool slice_fits(int64_t m, int64_t n, int eb) { return slice_config(m, n, eb, 1, nullptr).K > 0; }
+
+bool slice_group_params(int64_t m, int64_t n, int eb, const void *data, uint32_t *H, uint32_t *P, bool *vec) {
+  if (m < 2 || n < 2 || m > (1 << 24) || n > (1 << 24)) return false;
+  int64_t pitch = (n * eb + 15) / 16 * 16;
+  if ((pitch / 16) % 2 == 0) pitch += 16;
+  const int64_t rows = ((m + kSliceGroupK - 1) / kSliceGroupK + 31) / 32 * 32;
+  if (rows * pitch > kSliceSmemCap) return false;
+  *H = (uint32_t)rows;
+  *P = (uint32_t)pitch;
+  *vec = (n * eb) % 16 == 0 && (m * eb) % 16 == 0 && ((uintptr_t)data % 16) == 0;
+  return true;
+}
+
+int launch_slice_group(const void *entries, int32_t n_entries, int64_t n_items, int64_t smem, cudaStream_t st) {
+  if (n_items <= 0) return T213_OK;
+  auto kern = k_slice_group<true>;
+  int status = prep_kernel(kern, smem, kSliceGroupK);
+  if (status) return status;
+  const int res = clusters_resident((const void *)kern, kSliceThreads, smem, kSliceGroupK);
+  if (res < 1) return cuda_status(cudaErrorInvalidConfiguration, "slice group cluster cannot be resident");
+  const int64_t clusters = std::min<int64_t>(n_items, res);
+  return launch_k(kern, clusters * kSliceGroupK, kSliceThreads, smem, kSliceGroupK, st,
+                  (const SliceEntry *)entries, n_entries, n_items);
+}
 
 std::string describe_slice(int64_t m, int64_t n, int eb, int64_t d3) {
   SliceCfg c = slice_config(m, n, eb, d3, nullptr);
