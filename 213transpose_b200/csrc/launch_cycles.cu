@@ -81,7 +81,14 @@ int walk_and_chunk(const P &dst, int64_t S, int64_t items_per_chunk, std::vector
                    std::vector<CarryItem> &carries, int64_t &n_cycles, int64_t &moved, int64_t &max_len) {
   const DevInfo &d = dev_info();
   const int64_t resident_teams = (int64_t)d.sms * 8;
-  const int64_t target_chunks = std::max<int64_t>(1, 8 * resident_teams / std::max<int64_t>(1, items_per_chunk));
+  // T213_SEG_ITEMS: walker items per resident team (default 8); fewer means
+  // longer chunks and fewer carry slots, more means finer load balance
+  static const int64_t items_per_team = [] {
+    const char *v = std::getenv("T213_SEG_ITEMS");
+    return v && std::atoi(v) > 0 ? (int64_t)std::atoi(v) : (int64_t)8;
+  }();
+  const int64_t target_chunks =
+      std::max<int64_t>(1, items_per_team * resident_teams / std::max<int64_t>(1, items_per_chunk));
   const int64_t Lc = std::max<int64_t>(16, (S + target_chunks - 1) / target_chunks);
   std::vector<uint64_t> seen((size_t)((S + 63) / 64), 0);
   std::vector<int64_t> marks;

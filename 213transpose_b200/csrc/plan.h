@@ -63,8 +63,10 @@ struct GroupExec;
 GroupExec *group_exec_create(int64_t max_passes, int64_t max_items, size_t carry_bytes, int *status);
 void group_exec_destroy(GroupExec *g);
 // The plan a tensor takes inside the persistent kernel (the automatic choice,
-// else another family whose passes fit its shared memory); null if none fits.
-std::shared_ptr<Plan> group_plan(int64_t d1, int64_t d2, int64_t d3, int eb, int *status);
+// else the cheapest other family whose passes fit its shared memory); null if
+// none fits, and, unless search_slice, when the automatic choice is the
+// one-pass slice plan (which runs on its own launch).
+std::shared_ptr<Plan> group_plan(int64_t d1, int64_t d2, int64_t d3, int eb, int *status, bool search_slice);
 // Enqueues one k_batch launch over the tensors on st (tables copied from the
 // executor's pinned staging, counters reset), then copies the kernel's status
 // word to the executor's host mirror and records its event.  The executor's

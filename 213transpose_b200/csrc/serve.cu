@@ -358,7 +358,7 @@ class PlannerPool {
             get_plan(r.d1, r.d2, r.d3, r.elem_bytes, r.plan_kind, 0, &st);  // errors resurface at dispatch
             const int64_t bytes = r.d1 * r.d2 * r.d3 * r.elem_bytes;
             if (r.plan_kind == T213_PLAN_AUTO && bytes <= group_max_bytes)
-              groupable_[ri] = group_plan(r.d1, r.d2, r.d3, r.elem_bytes, &st) != nullptr;
+              groupable_[ri] = group_plan(r.d1, r.d2, r.d3, r.elem_bytes, &st, false) != nullptr;
           }
           planned_[ri].store(1, std::memory_order_release);
         }
