@@ -853,8 +853,7 @@ SliceCfg slice_config(int64_t m, int64_t n, int eb, int64_t d3, const void *data
       break;
     }
   if (!K) return c;
-  const int sms = dev_info().sms;
-  while (K < 8 && d3 * 2 * K <= sms && m / (2 * K) >= 32) K *= 2;
+  (void)d3;  // the launch widens the cluster when slices leave SMs idle
   c.K = K;
   c.H = (uint32_t)rows(K);
   c.P = (uint32_t)P;
@@ -900,14 +899,45 @@ std::string describe_slice(int64_t m, int64_t n, int eb, int64_t d3) {
 
 int launch_slice(char *data, int64_t d3, int64_t m, int64_t n, int eb, cudaStream_t st, LaunchStats *ls) {
   if (d3 <= 0 || m <= 0 || n <= 0) return T213_OK;
-  const SliceCfg c = slice_config(m, n, eb, d3, data);
-  if (!c.K) {
+  const SliceCfg c0 = slice_config(m, n, eb, d3, data);
+  if (!c0.K) {
     set_error("slice does not fit a cluster's shared memory");
     return T213_ERR_UNSUPPORTED;
   }
   int status = T213_ERR_UNSUPPORTED;
   auto go = [&](auto kern) {
-    if ((status = prep_kernel(kern, c.smem, c.K))) return;
+    // The cluster size: from the smallest that holds a slice, doubled (up to
+    // 8, with at least 32 rows per CTA) while that lowers waves x bytes per
+    // CTA, the time of a launch in which every slice costs one CTA's load
+    // and write of its share.  E.g. 16 slices of fp32 512 x 384 take 16
+    // clusters of 4 (one wave of 198 KB per CTA), not 16 clusters of 8,
+    // which would need two waves when 15 of them are resident.
+    SliceCfg c = c0;
+    auto cost = [&](const SliceCfg &x) -> double {
+      int res = 0;
+      if (x.K > 1) {
+        if (prep_kernel(kern, x.smem, x.K)) return 1e30;
+        res = clusters_resident((const void *)kern, kSliceThreads, x.smem, x.K);
+      } else {
+        if (prep_kernel(kern, x.smem, 1)) return 1e30;
+        occupancy_cached((const void *)kern, kSliceThreads, x.smem, 1, &res);
+        res *= dev_info().sms;
+      }
+      if (res < 1) return 1e30;
+      return (double)((d3 + res - 1) / res) * (double)x.smem;
+    };
+    double best = cost(c);
+    for (int K = c0.K * 2; K <= 8 && m / K >= 32; K *= 2) {
+      SliceCfg x = c0;
+      x.K = K;
+      x.H = (uint32_t)(((m + K - 1) / K + 31) / 32 * 32);
+      x.smem = (int64_t)x.H * x.P;
+      const double cx = cost(x);
+      if (cx < best) {
+        best = cx;
+        c = x;
+      }
+    }
     int64_t clusters = d3;
     if (c.K > 1) {
       const int res = clusters_resident((const void *)kern, kSliceThreads, c.smem, c.K);
@@ -925,13 +955,15 @@ int launch_slice(char *data, int64_t d3, int64_t m, int64_t n, int eb, cudaStrea
                       c.P);
     if (ls) ls->launches++;
   };
+  // a cluster kernel when the smallest cluster that holds a slice has more
+  // than one CTA, else (one CTA per slice) the plain form
   auto pick = [&](auto EBc) {
     constexpr int EB = decltype(EBc)::value;
-    if (c.vec) {
-      if (c.K > 1) go(k_slice<EB, true, true>);
+    if (c0.vec) {
+      if (c0.K > 1 || m / 2 >= 32) go(k_slice<EB, true, true>);
       else go(k_slice<EB, true, false>);
     } else {
-      if (c.K > 1) go(k_slice<EB, false, true>);
+      if (c0.K > 1 || m / 2 >= 32) go(k_slice<EB, false, true>);
       else go(k_slice<EB, false, false>);
     }
   };
