@@ -81,11 +81,15 @@ int walk_and_chunk(const P &dst, int64_t S, int64_t items_per_chunk, std::vector
                    std::vector<CarryItem> &carries, int64_t &n_cycles, int64_t &moved, int64_t &max_len) {
   const DevInfo &d = dev_info();
   const int64_t resident_teams = (int64_t)d.sms * 8;
-  // T213_SEG_ITEMS: walker items per resident team (default 8); fewer means
-  // longer chunks and fewer carry slots, more means finer load balance
+  // T213_SEG_ITEMS: walker items per resident team (default 2); fewer means
+  // longer chunks and fewer carry slots, more means finer load balance.
+  // Measured on B200 (whole transpose, ms, 8 / 3 / 2 / 1 items): fp32
+  // (8192, 6144, 4) 0.554 / 0.548 / 0.541 / 0.542; int32 (3, 2^22, 8) 0.294 /
+  // 0.290 / 0.287 / 0.288; 16-byte (92, 1173128, 1) 1.317 / 1.305 / 1.279 /
+  // 1.405; fp32 (2^24, 48, 1) 2.574 / 2.580 / 2.561 / 2.521.
   static const int64_t items_per_team = [] {
     const char *v = std::getenv("T213_SEG_ITEMS");
-    return v && std::atoi(v) > 0 ? (int64_t)std::atoi(v) : (int64_t)8;
+    return v && std::atoi(v) > 0 ? (int64_t)std::atoi(v) : (int64_t)2;
   }();
   const int64_t target_chunks =
       std::max<int64_t>(1, items_per_team * resident_teams / std::max<int64_t>(1, items_per_chunk));

@@ -735,13 +735,13 @@ std::shared_ptr<Plan> get_plan(int64_t d1, int64_t d2, int64_t d3, int eb, int k
       // The one-pass cluster plan (T213_PLAN_SLICE) wins where launch latency
       // dominates: small tensors whose rows are 16-byte multiples both ways.
       // Measured on B200: fp32 (256, 128, 64) 0.0126 ms against 0.0190 for
-      // BLOCKS; at 12 MB and above it only ties (fp32 (512, 384, 16) 0.0272
-      // against 0.0276).  Its element-wise form (other alignments) won on
-      // fp64 (45, 600, 2) (0.015 against 0.025 ms) but lost badly on 1-byte
+      // BLOCKS; fp32 (512, 384, 16) 0.0192 against 0.0244 (clusters of 4, one
+      // wave).  Its element-wise form (other alignments) won on fp64
+      // (45, 600, 2) (0.015 against 0.025 ms) but lost badly on 1-byte
       // (1000, 999, 1) (0.26 against 0.15 ms).  So it is ranked for tensors
-      // up to 8 MB with aligned rows only, and is otherwise taken when forced
-      // or chosen by the tuner.
-      if (slice_fits(m, n, eb) && (n * eb) % 16 == 0 && (m * eb) % 16 == 0 && d1 * d2 * d3 * eb <= (8ll << 20))
+      // up to 16 MB with aligned rows only, and is otherwise taken when
+      // forced or chosen by the tuner.
+      if (slice_fits(m, n, eb) && (n * eb) % 16 == 0 && (m * eb) % 16 == 0 && d1 * d2 * d3 * eb <= (16ll << 20))
         cands.push_back({T213_PLAN_SLICE, 0, 1.0});
       // The Catanzaro decomposition both ways: the reference's dispatcher
       // takes C2R when d1 >= d2, else R2C (src/transpose.cu:117-123); here

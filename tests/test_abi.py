@@ -73,7 +73,7 @@ CONFIG_PLANS = [
     # (d1, d2, d3, eb): expected plan family of the dispatcher
     ((8192, 6144, 4, 4), "blocks t=2048"),
     ((7919, 6151, 2, 8), "c2r"),
-    ((512, 384, 16, 4), "blocks t=128"),
+    ((512, 384, 16, 4), "slice: slice("),
     ((32, 1 << 24, 1, 4), "bands t="),
     ((1 << 24, 48, 1, 4), "bands_t t="),
     ((3, 1 << 22, 8, 4), "bands t="),
