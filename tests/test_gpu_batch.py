@@ -84,6 +84,15 @@ def test_batch_full_config_round_trip(cuda, t213):
         d1, d2, d3, eb, _ = shapes[i]
         want = origs[i].view(d3, d2, d1, eb).permute(0, 2, 1, 3).contiguous().view(-1)
         assert cuda.equal(devs[i], want), shapes[i]
+    # and a sample of 24 (the three largest among them) byte for byte against the oracle
+    from oracle import oracle as O
+    size = [d1 * d2 * d3 * eb for d1, d2, d3, eb, _ in shapes]
+    largest = sorted(range(512), key=lambda i: -size[i])[:3]
+    for i in sorted(set(largest) | set(range(5, 512, 23))):
+        d1, d2, d3, eb, _ = shapes[i]
+        x = origs[i].cpu().numpy()
+        want = O.gather213(x.view(np.dtype((np.void, eb))), d1, d2, d3).view(np.uint8)
+        assert np.array_equal(from_device(devs[i]), want), shapes[i]
     back.execute()
     assert back.status() == 0
     bad = [shapes[i] for i in range(512) if not cuda.equal(devs[i], origs[i])]
