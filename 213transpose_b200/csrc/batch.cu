@@ -249,6 +249,8 @@ int build_batch_tables(const t213_tensor_desc *tensors, int32_t count, const std
           bp.W = W;
           bp.WS = WS;
           bp.n_strips = (q.n + W - 1) / W;
+          bp.div_w = FastDiv<uint32_t>((uint64_t)(W / (bp.aw / eb)));
+          bp.div_wl = FastDiv<uint32_t>((uint64_t)((q.n - (bp.n_strips - 1) * W) / (bp.aw / eb)));
           bp.n_units = d.d3 * bp.n_strips;
           bp.u64 = !fits32(q.fn, q.m, q.n);
           if (bp.u64)
@@ -262,6 +264,8 @@ int build_batch_tables(const t213_tensor_desc *tensors, int32_t count, const std
           bp.aw = aw_for(eb, data, q.n * eb);
           bp.rows_per_unit = std::max<int64_t>(1, std::min<int64_t>(q.m, (64 * 1024) / std::max<int64_t>(1, q.n * eb)));
           bp.n_units = (d.d3 * q.m + bp.rows_per_unit - 1) / bp.rows_per_unit;
+          bp.div_w = FastDiv<uint32_t>((uint64_t)(q.n / (bp.aw / eb)));
+          bp.div_m = FastDiv<uint64_t>((uint64_t)q.m);
           bp.u64 = !fits32(q.fn, q.m, q.n);
           if (bp.u64)
             set_row_fn<uint64_t>(bp.f64, q.fn);

@@ -111,6 +111,8 @@ struct BPass {
   int64_t n_chunks = 0, n_carry = 0, seg_bytes = 0, piece_bytes = 0, pieces = 0;
   int32_t seg_tma = 0, seg_aw = 16;
   int64_t n_units = 0;
+  FastDiv<uint32_t> div_w, div_wl;  // COL: words per row of a full / the last strip; ROW: words per row
+  FastDiv<uint64_t> div_m;          // ROW: m
   int32_t done_ctr = 0, dep_ctr = -1;
   int64_t dep_target = 0;
   AnyFn<uint32_t> f32;
@@ -305,31 +307,51 @@ __device__ __noinline__ void bx_band(const BPass &P, int64_t u0, int64_t u1, uns
 }
 
 // ------------------------------------------------------------------- COL ----
-template <int EB, int AW, typename U>
-__device__ __noinline__ void bx_col(const BPass &P, const AnyFn<U> &f, int64_t u0, int64_t u1,
-                                    unsigned char *smem) {
+// The functor type F is a template parameter (the dispatcher switches on the
+// kind once per item), and every division by a per-pass constant goes
+// through a FastDiv the host computed, so the per-element work is the
+// functor's own arithmetic, one shared-memory read and the store.
+template <typename T>
+struct TypeTag {
+  using type = T;
+};
+
+template <typename U>
+__device__ __forceinline__ const AnyFn<U> &any_fn(const BPass &P);
+template <>
+__device__ __forceinline__ const AnyFn<uint32_t> &any_fn<uint32_t>(const BPass &P) {
+  return P.f32;
+}
+template <>
+__device__ __forceinline__ const AnyFn<uint64_t> &any_fn<uint64_t>(const BPass &P) {
+  return P.f64;
+}
+
+template <int EB, int AW, typename U, typename F>
+__device__ __noinline__ void bx_col(const BPass &P, int64_t u0, int64_t u1, unsigned char *smem) {
   using E = typename ElemT<EB>::type;
   using Wd = typename WordT<AW>::type;
   using PK = Pack<AW, EB>;
   constexpr int PER = AW / EB;
+  const F fn = any_fn<U>(P).template as<F>();
   const U m = (U)P.m, n = (U)P.n, W = (U)P.W, WS = (U)P.WS;
+  const FastDiv<uint32_t> dfull = P.div_w, dlast = P.div_wl;  // words per row of a full / the last strip
   const int64_t pitch = P.n * EB;
-  auto strip = [&](int64_t u, U &j0, uint32_t &wpr, char *&sbase) {
+  auto strip = [&](int64_t u, U &j0, FastDiv<uint32_t> &wd, char *&sbase) {
     const int64_t k = u / P.n_strips;
     const U s = (U)(u - k * P.n_strips);
     j0 = s * W;
-    const U wn = min(W, n - j0);
-    wpr = (uint32_t)(wn / PER);
+    wd = j0 + W <= n ? dfull : dlast;
     sbase = P.data + (k * (int64_t)m * n + j0) * EB;
   };
   auto stage = [&](int64_t u, E *sm) {
     U j0;
-    uint32_t wpr;
+    FastDiv<uint32_t> wd;
     char *sbase;
-    strip(u, j0, wpr, sbase);
-    const uint32_t nw = (uint32_t)m * wpr;
+    strip(u, j0, wd, sbase);
+    const uint32_t wpr = wd.get(), nw = (uint32_t)m * wpr;
     for (uint32_t t = threadIdx.x; t < nw; t += blockDim.x) {
-      const uint32_t r = t / wpr, w = t - r * wpr;
+      const uint32_t r = wd.div(t), w = t - r * wpr;
       const Wd *gp = reinterpret_cast<const Wd *>(sbase + (int64_t)r * pitch) + w;
       if constexpr (AW >= 4)
         cp_async<AW>(reinterpret_cast<Wd *>(sm + (int64_t)r * WS) + w, gp);
@@ -349,16 +371,16 @@ __device__ __noinline__ void bx_col(const BPass &P, const AnyFn<U> &f, int64_t u
     }
     __syncthreads();
     U j0;
-    uint32_t wpr;
+    FastDiv<uint32_t> wd;
     char *sbase;
-    strip(u, j0, wpr, sbase);
-    const uint32_t nw = (uint32_t)m * wpr;
+    strip(u, j0, wd, sbase);
+    const uint32_t wpr = wd.get(), nw = (uint32_t)m * wpr;
     for (uint32_t t = threadIdx.x; t < nw; t += blockDim.x) {
-      const uint32_t r = t / wpr, w = t - r * wpr;
+      const uint32_t r = wd.div(t), w = t - r * wpr;
       typename PK::U pk;
 #pragma unroll
       for (int e = 0; e < PER; e++) {
-        const U si = f.col((U)r, j0 + w * PER + e);
+        const U si = fn((U)r, j0 + w * PER + e);
         pk.e[e] = sm[(int64_t)si * WS + w * PER + e];
       }
       __stcs(reinterpret_cast<Wd *>(sbase + (int64_t)r * pitch) + w, pk.w);
@@ -368,16 +390,18 @@ __device__ __noinline__ void bx_col(const BPass &P, const AnyFn<U> &f, int64_t u
 }
 
 // ------------------------------------------------------------------- ROW ----
-template <int EB, int AW, typename U>
-__device__ __noinline__ void bx_row(const BPass &P, const AnyFn<U> &f, int64_t u0, int64_t u1,
-                                    unsigned char *smem) {
+template <int EB, int AW, typename U, typename F>
+__device__ __noinline__ void bx_row(const BPass &P, int64_t u0, int64_t u1, unsigned char *smem) {
   using E = typename ElemT<EB>::type;
   using Wd = typename WordT<AW>::type;
   using PK = Pack<AW, EB>;
   constexpr int PER = AW / EB;
+  const F fn = any_fn<U>(P).template as<F>();
   const U m = (U)P.m, n = (U)P.n;
+  const FastDiv<uint32_t> wd = P.div_w;  // words per row
+  const FastDiv<uint64_t> md = P.div_m;  // m
+  const uint32_t wpr = wd.get();
   const int64_t total_rows = P.d3 * P.m;
-  const uint32_t wpr = (uint32_t)(n / PER);
   auto stage = [&](int64_t u, E *sm) {
     const int64_t r0 = u * P.rows_per_unit;
     const int nr = (int)min((int64_t)P.rows_per_unit, total_rows - r0);
@@ -405,14 +429,15 @@ __device__ __noinline__ void bx_row(const BPass &P, const AnyFn<U> &f, int64_t u
     const int nr = (int)min((int64_t)P.rows_per_unit, total_rows - r0);
     Wd *g = reinterpret_cast<Wd *>(P.data + r0 * (int64_t)n * EB);
     const uint32_t nw = (uint32_t)nr * wpr;
-    const int64_t i_base = r0 % (int64_t)m;
+    const uint64_t i_base = md.mod((uint64_t)r0);
     for (uint32_t w = threadIdx.x; w < nw; w += blockDim.x) {
-      const uint32_t rr = w / wpr;
+      const uint32_t rr = wd.div(w);
       const U j0 = (U)(w - rr * wpr) * PER;
-      const U i = (U)((i_base + rr) % (int64_t)m);
+      const uint64_t ii = i_base + rr;
+      const U i = (U)(ii < (uint64_t)m ? ii : md.mod(ii));
       typename PK::U pk;
 #pragma unroll
-      for (int e = 0; e < PER; e++) pk.e[e] = sm[(int64_t)rr * n + f.row(i, j0 + e)];
+      for (int e = 0; e < PER; e++) pk.e[e] = sm[(int64_t)rr * n + fn(i, j0 + e)];
       __stcs(g + w, pk.w);
     }
     __syncthreads();
@@ -611,28 +636,50 @@ __device__ bool bx_dispatch(const BPass &P, const AnyFn<U> &f, int64_t u0, int64
         default: bx_band<16, false>(P, u0, u1, smem); break;
       }
       return true;
-    case BK_COL:
-      switch (P.eb * 100 + P.aw) {
-        case 101: bx_col<1, 1, U>(P, f, u0, u1, smem); break;
-        case 202: bx_col<2, 2, U>(P, f, u0, u1, smem); break;
-        case 404: bx_col<4, 4, U>(P, f, u0, u1, smem); break;
-        case 416: bx_col<4, 16, U>(P, f, u0, u1, smem); break;
-        case 808: bx_col<8, 8, U>(P, f, u0, u1, smem); break;
-        case 816: bx_col<8, 16, U>(P, f, u0, u1, smem); break;
-        default: bx_col<16, 16, U>(P, f, u0, u1, smem); break;
+    case BK_COL: {
+      auto go = [&](auto tag) {
+        using F = typename decltype(tag)::type;
+        switch (P.eb * 100 + P.aw) {
+          case 101: bx_col<1, 1, U, F>(P, u0, u1, smem); break;
+          case 202: bx_col<2, 2, U, F>(P, u0, u1, smem); break;
+          case 404: bx_col<4, 4, U, F>(P, u0, u1, smem); break;
+          case 416: bx_col<4, 16, U, F>(P, u0, u1, smem); break;
+          case 808: bx_col<8, 8, U, F>(P, u0, u1, smem); break;
+          case 816: bx_col<8, 16, U, F>(P, u0, u1, smem); break;
+          default: bx_col<16, 16, U, F>(P, u0, u1, smem); break;
+        }
+      };
+      switch (f.kind) {
+        case T213_FN_C2R_PREROTATOR: go(TypeTag<RotGather<U, RotC2RPre<U>>>{}); break;
+        case T213_FN_C2R_POSTROTATOR: go(TypeTag<RotGather<U, RotC2RPost<U>>>{}); break;
+        case T213_FN_R2C_PREROTATOR: go(TypeTag<RotGather<U, RotR2CPre<U>>>{}); break;
+        case T213_FN_R2C_POSTROTATOR: go(TypeTag<RotGather<U, RotR2CPost<U>>>{}); break;
+        case T213_FN_C2R_FUSED_PREOP: go(TypeTag<ColC2RFusedPre<U>>{}); break;
+        case T213_FN_C2R_FUSED_POSTOP: go(TypeTag<ColC2RFusedPost<U>>{}); break;
+        case T213_FN_R2C_FUSED_PREOP: go(TypeTag<ColR2CFusedPre<U>>{}); break;
+        default: go(TypeTag<ColR2CFusedPost<U>>{}); break;
       }
       return true;
-    case BK_ROW:
-      switch (P.eb * 100 + P.aw) {
-        case 101: bx_row<1, 1, U>(P, f, u0, u1, smem); break;
-        case 202: bx_row<2, 2, U>(P, f, u0, u1, smem); break;
-        case 404: bx_row<4, 4, U>(P, f, u0, u1, smem); break;
-        case 416: bx_row<4, 16, U>(P, f, u0, u1, smem); break;
-        case 808: bx_row<8, 8, U>(P, f, u0, u1, smem); break;
-        case 816: bx_row<8, 16, U>(P, f, u0, u1, smem); break;
-        default: bx_row<16, 16, U>(P, f, u0, u1, smem); break;
-      }
+    }
+    case BK_ROW: {
+      auto go = [&](auto tag) {
+        using F = typename decltype(tag)::type;
+        switch (P.eb * 100 + P.aw) {
+          case 101: bx_row<1, 1, U, F>(P, u0, u1, smem); break;
+          case 202: bx_row<2, 2, U, F>(P, u0, u1, smem); break;
+          case 404: bx_row<4, 4, U, F>(P, u0, u1, smem); break;
+          case 416: bx_row<4, 16, U, F>(P, u0, u1, smem); break;
+          case 808: bx_row<8, 8, U, F>(P, u0, u1, smem); break;
+          case 816: bx_row<8, 16, U, F>(P, u0, u1, smem); break;
+          default: bx_row<16, 16, U, F>(P, u0, u1, smem); break;
+        }
+      };
+      if (f.kind == T213_FN_R2C_SHUFFLE)
+        go(TypeTag<RowR2CShuffle<U>>{});
+      else
+        go(TypeTag<RowC2RShuffle<U>>{});
       return true;
+    }
     case BK_CARRY:
       bx_carry(P, u0, u1);
       return true;
