@@ -118,6 +118,89 @@ __global__ void __launch_bounds__(kGatherThreads)
 }
 
 // ---------------------------------------------------------------------------
+// Row gather with 16-byte global accesses for rows whose pitch is not a
+// multiple of 16 bytes (4-byte elements in rows of odd length, and the like).
+// A unit of consecutive rows is one contiguous byte range [b0, b1).  The CTA
+// loads the 16-byte blocks that cover it with 16-byte cp.async: up to 15 bytes
+// on each side belong to the neighbouring units (or lie past the tensor in
+// the same 16-byte block, so in the same page); they are read and never used.
+// It writes the range back as 16-byte stores between the first and the last
+// 16-byte boundary inside it, and as single elements before and after.  A
+// thread takes 16/EB consecutive output elements, finds the row and column of
+// the first with one division and steps the rest.
+// ---------------------------------------------------------------------------
+template <int EB, typename F, typename U>
+__global__ void __launch_bounds__(kGatherThreads)
+    k_row_gather_peel(char *__restrict__ data, int64_t total_rows, U m, U n, int rows_per_unit, FastDiv<U> ndiv,
+                      FastDiv<U> mdiv, F fn) {
+  using E = typename ElemT<EB>::type;
+  constexpr int PER = 16 / EB;
+  static_assert(EB < 16, "16-byte elements are always 16-byte aligned");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const E *sm = reinterpret_cast<const E *>(smem_raw);
+  const int64_t n_units = (total_rows + rows_per_unit - 1) / rows_per_unit;
+  const int64_t row_bytes = (int64_t)n * EB;
+  for (int64_t u = blockIdx.x; u < n_units; u += gridDim.x) {
+    const int64_t r0 = u * rows_per_unit;
+    const int64_t nr = min((int64_t)rows_per_unit, total_rows - r0);
+    const uintptr_t b0 = reinterpret_cast<uintptr_t>(data + r0 * row_bytes);
+    const uintptr_t b1 = b0 + (uintptr_t)(nr * row_bytes);
+    const uintptr_t a0 = b0 & ~(uintptr_t)15, a1 = (b1 + 15) & ~(uintptr_t)15;
+    {
+      const uint32_t nv = (uint32_t)((a1 - a0) >> 4);
+      const uint4 *g = reinterpret_cast<const uint4 *>(a0);
+#pragma unroll 4
+      for (uint32_t v = threadIdx.x; v < nv; v += blockDim.x) cp_async<16>(smem_raw + 16 * (size_t)v, g + v);
+      cp_async_wait_all();
+    }
+    __syncthreads();
+    const U d0 = (U)((b0 - a0) / EB);  // unit element 0 sits at sm[d0]
+    const U i_base = (U)(r0 % (int64_t)m);
+    const U total = (U)(nr * (int64_t)n);
+    // value of unit element q = rr * n + j
+    auto value = [&](U rr, U j, U i) -> E { return sm[d0 + rr * n + fn(i, j)]; };
+    auto locate = [&](U q, U &rr, U &j, U &i) {
+      rr = ndiv.div(q);
+      j = q - rr * n;
+      const U ii = i_base + rr;
+      i = ii < m ? ii : mdiv.mod(ii);
+    };
+    // 16-byte stores over [c0, c1)
+    const uintptr_t c0 = min((b0 + 15) & ~(uintptr_t)15, b1), c1 = max(b1 & ~(uintptr_t)15, c0);
+    const U qh = (U)((c0 - b0) / EB), qt = (U)((c1 - b0) / EB);
+    const uint32_t nvec = (uint32_t)((c1 - c0) >> 4);
+    uint4 *gout = reinterpret_cast<uint4 *>(c0);
+    for (uint32_t v = threadIdx.x; v < nvec; v += blockDim.x) {
+      U rr, j, i;
+      locate(qh + (U)v * PER, rr, j, i);
+      union {
+        uint4 w;
+        E e[PER];
+      } pk;
+#pragma unroll
+      for (int e = 0; e < PER; e++) {
+        pk.e[e] = value(rr, j, i);
+        if (++j == n) {
+          j = 0;
+          rr++;
+          if (++i == m) i = 0;
+        }
+      }
+      __stcs(gout + v, pk.w);
+    }
+    // single elements before c0 and from c1 on
+    const U nhead = qh, ntail = total - qt;
+    for (U t = threadIdx.x; t < nhead + ntail; t += blockDim.x) {
+      const U q = t < nhead ? t : qt + (t - nhead);
+      U rr, j, i;
+      locate(q, rr, j, i);
+      reinterpret_cast<E *>(b0)[q] = value(rr, j, i);
+    }
+    __syncthreads();  // shared memory is restaged by the next unit
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Row gather with the next unit's load in flight: a unit (one or more whole
 // rows, at most half the CTA's shared memory) is copied into one of two
 // buffers with cp.async groups while the previous unit is gathered from the
