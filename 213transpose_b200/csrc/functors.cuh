@@ -183,6 +183,46 @@ struct RowR2CShuffle {  // equations.h:178-194
   }
 };
 
+// Row shufflers evaluated along a row, at (i, j), (i, j + 1), ...: when m and
+// n are coprime both shuffles step by a constant modulo n (C2R: s = k (j - i)
+// mod n grows by k; R2C: s = (i + j m) mod n grows by m mod n), so the next
+// value is an add and a conditional subtract.  Other row functors, and the
+// shuffles of non-coprime shapes, are evaluated anew.
+template <typename F, typename U>
+struct RowStepper {
+  const F &f;
+  T213_HD explicit RowStepper(const F &f_) : f(f_) {}
+  T213_HD U next(U, U i, U j) const { return f(i, j); }
+};
+
+template <typename U>
+struct RowStepper<RowC2RShuffle<U>, U> {
+  const RowC2RShuffle<U> &f;
+  U inc, n;
+  bool on;
+  T213_HD explicit RowStepper(const RowC2RShuffle<U> &f_)
+      : f(f_), inc(f_.k), n(f_.n.get()), on(f_.c.get() == 1) {}
+  T213_HD U next(U s, U i, U j) const {
+    if (!on) return f(i, j);
+    const U t = s + inc;
+    return t >= n ? t - n : t;
+  }
+};
+
+template <typename U>
+struct RowStepper<RowR2CShuffle<U>, U> {
+  const RowR2CShuffle<U> &f;
+  U inc, n;
+  bool on;
+  T213_HD explicit RowStepper(const RowR2CShuffle<U> &f_)
+      : f(f_), inc(f_.n.mod(f_.m.get())), n(f_.n.get()), on(f_.b.get() == f_.n.get()) {}
+  T213_HD U next(U s, U i, U j) const {
+    if (!on) return f(i, j);
+    const U t = s + inc;
+    return t >= n ? t - n : t;
+  }
+};
+
 // ------------------------------------------------------------ row scatters --
 // new[dst(i)][*] = old[i][*]
 

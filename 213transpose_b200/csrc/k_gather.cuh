@@ -170,6 +170,7 @@ __global__ void __launch_bounds__(kGatherThreads)
     const U qh = (U)((c0 - b0) / EB), qt = (U)((c1 - b0) / EB);
     const uint32_t nvec = (uint32_t)((c1 - c0) >> 4);
     uint4 *gout = reinterpret_cast<uint4 *>(c0);
+    const RowStepper<F, U> step(fn);
     for (uint32_t v = threadIdx.x; v < nvec; v += blockDim.x) {
       U rr, j, i;
       locate(qh + (U)v * PER, rr, j, i);
@@ -177,14 +178,20 @@ __global__ void __launch_bounds__(kGatherThreads)
         uint4 w;
         E e[PER];
       } pk;
+      U s = fn(i, j);
 #pragma unroll
       for (int e = 0; e < PER; e++) {
-        pk.e[e] = value(rr, j, i);
-        if (++j == n) {
-          j = 0;
-          rr++;
-          if (++i == m) i = 0;
+        if (e > 0) {
+          if (++j == n) {  // the word runs into the next row
+            j = 0;
+            rr++;
+            if (++i == m) i = 0;
+            s = fn(i, j);
+          } else {
+            s = step.next(s, i, j);
+          }
         }
+        pk.e[e] = sm[d0 + rr * n + s];
       }
       __stcs(gout + v, pk.w);
     }
