@@ -257,6 +257,36 @@ int build_batch_tables(const t213_tensor_desc *tensors, int32_t count, const std
             set_col_fn<uint64_t>(bp.f64, q.fn, q.m);
           else
             set_col_fn<uint32_t>(bp.f32, q.fn, q.m);
+          // the cluster-local form: forms 2 and 3 carry the row permuter in
+          // place of the functor (their key offsets are +-j mod m); at most
+          // 256 columns per strip (the offsets' shared-memory table)
+          bp.col_form = W <= kBatchAuxInts && std::getenv("T213_BATCH_COL_GENERIC") == nullptr
+                            ? col_local_form(q.fn, q.m)
+                            : 0;
+          if (bp.col_form == 2 || bp.col_form == 3) {
+            int64_t cc, qq;
+            if (bp.col_form == 2) {  // p = {m, n', c}: inverse post-permuter, q = b^-1 mod a
+              cc = q.fn.p[2] > 0 ? q.fn.p[2] : 1;
+              const int64_t a = q.m / cc, b = q.fn.p[1] / cc;
+              qq = 0;
+              if (a > 1) {
+                ext_gcd(b % a, a, &qq);
+                qq %= a;
+                if (qq < 0) qq += a;
+              }
+            } else {  // p = {a, c, m, q}: the pre-permuter
+              cc = q.fn.p[1] > 0 ? q.fn.p[1] : 1;
+              const int64_t a = q.fn.p[0] > 0 ? q.fn.p[0] : 1;
+              qq = ((q.fn.p[3] % a) + a) % a;
+            }
+            if (bp.u64)
+              bp.f64.set(T213_FN_R2C_PREPERMUTER, PermR2CPre<uint64_t>(q.m, cc, qq));
+            else
+              bp.f32.set(T213_FN_R2C_PREPERMUTER, PermR2CPre<uint32_t>(q.m, cc, qq));
+          }
+          bp.div_m = FastDiv<uint64_t>((uint64_t)q.m);
+          bp.div_m32 = FastDiv<uint32_t>((uint64_t)q.m);
+          if (bp.col_form && bp.aw < 16) bp.WS = bp.W;  // the diagonal reads are conflict-free unpadded
           break;
         }
         case PT_ROW: {

@@ -138,6 +138,12 @@ int launch_col_gather(const FnSpec &f, char *data, int64_t d3, int64_t m, int64_
 // Row gather new[i][j] = old[i][f(i,j)].
 int launch_row_gather(const FnSpec &f, char *data, int64_t d3, int64_t m, int64_t n, int eb,
                       cudaStream_t st, LaunchStats *ls);
+// Which cluster-local form a column functor with these parameters has (the
+// column kernels evaluate it as key offsets and row maps): 1 offsets of the
+// functor itself with identity maps, 2 the C2R fused post-op (+j offsets,
+// output rows through the inverse post-permuter), 3 the R2C fused pre-op (-j
+// offsets, source rows through the pre-permuter); 0 none.
+int col_local_form(const FnSpec &f, int64_t m);
 // Describes the variant launch_col_gather / launch_row_gather would pick.
 std::string describe_col_gather(int64_t m, int64_t n, int eb, const void *data);
 // The variant launch_col_gather picks for this functor (the cluster-local

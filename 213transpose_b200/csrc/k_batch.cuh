@@ -45,7 +45,8 @@ constexpr int kBatchWarps = kBatchThreads / 32;
 constexpr int kBatchRing = 6;                 // TMA buffers per walker warp
 constexpr int64_t kBatchPiece = 2048;         // bytes per TMA walker piece
 constexpr int64_t kBatchSmem = 192 * 1024;    // dynamic shared memory per CTA
-constexpr int64_t kBatchBarBytes = 1024;      // mbarriers live at the front
+constexpr int64_t kBatchBarBytes = 2048;      // mbarriers (first KB) and per-strip column offsets (second KB)
+constexpr int kBatchAuxInts = 256;            // column offsets of one strip (W <= 256)
 
 enum BKind { BK_TILE = 1, BK_BAND = 2, BK_COL = 3, BK_ROW = 4, BK_CARRY = 5, BK_SEG = 6 };
 
@@ -104,6 +105,7 @@ struct BPass {
   int64_t rows_per_unit = 0;               // ROW
   int64_t t = 0, Bm = 0, Bn = 0, nt = 0, pairs = 0;  // TILE
   int32_t tile_vec = 0, band_vec = 0;
+  int32_t col_form = 0;                    // COL: cluster-local form 1-3 of the functor, 0 = evaluate it per element
   int64_t R = 0, C = 0;                    // BAND
   const Chunk *chunks = nullptr;           // SEG / CARRY
   const CarryItem *carries = nullptr;
@@ -112,7 +114,8 @@ struct BPass {
   int32_t seg_tma = 0, seg_aw = 16;
   int64_t n_units = 0;
   FastDiv<uint32_t> div_w, div_wl;  // COL: words per row of a full / the last strip; ROW: words per row
-  FastDiv<uint64_t> div_m;          // ROW: m
+  FastDiv<uint64_t> div_m;          // ROW, COL: m
+  FastDiv<uint32_t> div_m32;        // COL: m, for 32-bit indices
   int32_t done_ctr = 0, dep_ctr = -1;
   int64_t dep_target = 0;
   AnyFn<uint32_t> f32;
@@ -327,6 +330,17 @@ __device__ __forceinline__ const AnyFn<uint64_t> &any_fn<uint64_t>(const BPass &
   return P.f64;
 }
 
+template <typename U>
+__device__ __forceinline__ FastDiv<U> pass_mdiv(const BPass &P);
+template <>
+__device__ __forceinline__ FastDiv<uint32_t> pass_mdiv<uint32_t>(const BPass &P) {
+  return P.div_m32;
+}
+template <>
+__device__ __forceinline__ FastDiv<uint64_t> pass_mdiv<uint64_t>(const BPass &P) {
+  return P.div_m;
+}
+
 template <int EB, int AW, typename U, typename F>
 __device__ __noinline__ void bx_col(const BPass &P, int64_t u0, int64_t u1, unsigned char *smem) {
   using E = typename ElemT<EB>::type;
@@ -386,6 +400,104 @@ __device__ __noinline__ void bx_col(const BPass &P, int64_t u0, int64_t u1, unsi
       __stcs(reinterpret_cast<Wd *>(sbase + (int64_t)r * pitch) + w, pk.w);
     }
     __syncthreads();
+  }
+}
+
+// COL items whose functor has a cluster-local form (the form k_col_local
+// uses, with the whole strip in this CTA): column w of a strip has a key offset
+// r_w, slot s of the staged strip holds source row Fm(s), and output row Gm(o)
+// takes column w from slot (o + r_w) mod m.  The functor is evaluated once per
+// column, the row maps once per row, and an element costs an add and a shared
+// read.  A lane keeps one word of the rows it writes, so its offsets stay in
+// registers.
+template <int EB, int AW, typename U, typename Off, typename Fm, typename Gm>
+__device__ __noinline__ void bx_col_local(const BPass &P, const Off off, const Fm F, const Gm G, int64_t u0, int64_t u1,
+                                          unsigned char *smem, int *s_sh) {
+  using E = typename ElemT<EB>::type;
+  using Wd = typename WordT<AW>::type;
+  using PK = Pack<AW, EB>;
+  constexpr int PER = AW / EB;
+  const U m = (U)P.m, n = (U)P.n, W = (U)P.W, WS = (U)P.WS;
+  const FastDiv<uint32_t> dfull = P.div_w, dlast = P.div_wl;
+  const int64_t pitch = P.n * EB;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  auto strip = [&](int64_t u, U &j0, FastDiv<uint32_t> &wd, char *&sbase) {
+    const int64_t k = u / P.n_strips;
+    const U s = (U)(u - k * P.n_strips);
+    j0 = s * W;
+    wd = j0 + W <= n ? dfull : dlast;
+    sbase = P.data + (k * (int64_t)m * n + j0) * EB;
+  };
+  auto stage = [&](int64_t u, E *sm) {
+    U j0;
+    FastDiv<uint32_t> wd;
+    char *sbase;
+    strip(u, j0, wd, sbase);
+    const uint32_t wpr = wd.get(), nw = (uint32_t)m * wpr;
+    for (uint32_t t = threadIdx.x; t < nw; t += blockDim.x) {
+      const uint32_t sl = wd.div(t), w = t - sl * wpr;
+      const Wd *gp = reinterpret_cast<const Wd *>(sbase + (int64_t)F((U)sl) * pitch) + w;
+      if constexpr (AW >= 4)
+        cp_async<AW>(reinterpret_cast<Wd *>(sm + (int64_t)sl * WS) + w, gp);
+      else
+        reinterpret_cast<Wd *>(sm + (int64_t)sl * WS)[w] = *gp;
+    }
+    cp_async_commit();
+  };
+  stage(u0, reinterpret_cast<E *>(smem));
+  for (int64_t u = u0; u < u1; u++) {
+    E *sm = reinterpret_cast<E *>(smem + ((u - u0) & 1) * kBatchHalf);
+    if (u + 1 < u1) {
+      stage(u + 1, reinterpret_cast<E *>(smem + ((u + 1 - u0) & 1) * kBatchHalf));
+      cp_async_wait_group<1>();
+    } else {
+      cp_async_wait_group<0>();
+    }
+    U j0;
+    FastDiv<uint32_t> wd;
+    char *sbase;
+    strip(u, j0, wd, sbase);
+    const uint32_t wpr = wd.get(), wn = wpr * PER;
+    for (uint32_t w = threadIdx.x; w < wn; w += blockDim.x) s_sh[w] = (int)off(j0 + w);
+    __syncthreads();  // the strip has landed and its offsets are in place
+    auto slot = [&](U o, U r) -> U {
+      const U v = o + r;
+      return v >= m ? v - m : v;
+    };
+    if (32 % wpr == 0) {
+      const uint32_t rpi = 32 / wpr, lr = lane / wpr, lw = lane - lr * wpr;
+      U sh[PER];
+#pragma unroll
+      for (int e = 0; e < PER; e++) sh[e] = (U)s_sh[lw * PER + e];
+      for (U ob = (U)warp * 32; ob < m; ob += (U)nwarps * 32) {
+        const U myo = ob + lane;
+        const U myrow = myo < m ? G(myo) : 0;
+        for (uint32_t r = lr; r < 32; r += rpi) {
+          const U row = __shfl_sync(0xffffffffu, myrow, r);
+          const U o = ob + r;
+          if (o < m) {
+            typename PK::U pk;
+#pragma unroll
+            for (int e = 0; e < PER; e++) pk.e[e] = sm[(int64_t)slot(o, sh[e]) * WS + lw * PER + e];
+            __stcs(reinterpret_cast<Wd *>(sbase + (int64_t)row * pitch) + lw, pk.w);
+          }
+        }
+      }
+    } else {
+      const uint32_t nw = (uint32_t)m * wpr;
+      for (uint32_t t = threadIdx.x; t < nw; t += blockDim.x) {
+        const uint32_t o = wd.div(t), w = t - o * wpr;
+        const U row = G((U)o);
+        typename PK::U pk;
+#pragma unroll
+        for (int e = 0; e < PER; e++) {
+          const uint32_t c = w * PER + e;
+          pk.e[e] = sm[(int64_t)slot((U)o, (U)s_sh[c]) * WS + c];
+        }
+        __stcs(reinterpret_cast<Wd *>(sbase + (int64_t)row * pitch) + w, pk.w);
+      }
+    }
+    __syncthreads();  // the buffer is restaged two strips on, the offsets by the next strip
   }
 }
 
@@ -637,6 +749,50 @@ __device__ bool bx_dispatch(const BPass &P, const AnyFn<U> &f, int64_t u0, int64
       }
       return true;
     case BK_COL: {
+      if (P.col_form) {
+        int *s_sh = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(bars) + 1024);
+        auto loc = [&](auto off, auto F, auto G) {
+          using Off = decltype(off);
+          using Fm = decltype(F);
+          using Gm = decltype(G);
+          switch (P.eb * 100 + P.aw) {
+            case 101: bx_col_local<1, 1, U, Off, Fm, Gm>(P, off, F, G, u0, u1, smem, s_sh); break;
+            case 202: bx_col_local<2, 2, U, Off, Fm, Gm>(P, off, F, G, u0, u1, smem, s_sh); break;
+            case 404: bx_col_local<4, 4, U, Off, Fm, Gm>(P, off, F, G, u0, u1, smem, s_sh); break;
+            case 416: bx_col_local<4, 16, U, Off, Fm, Gm>(P, off, F, G, u0, u1, smem, s_sh); break;
+            case 808: bx_col_local<8, 8, U, Off, Fm, Gm>(P, off, F, G, u0, u1, smem, s_sh); break;
+            case 816: bx_col_local<8, 16, U, Off, Fm, Gm>(P, off, F, G, u0, u1, smem, s_sh); break;
+            default: bx_col_local<16, 16, U, Off, Fm, Gm>(P, off, F, G, u0, u1, smem, s_sh); break;
+          }
+        };
+        if (P.col_form == 2) {
+          loc(OffAffine<U, false>{pass_mdiv<U>(P)}, MapId<U>{}, f.template as<PermR2CPre<U>>());
+        } else if (P.col_form == 3) {
+          loc(OffAffine<U, true>{pass_mdiv<U>(P)}, f.template as<PermR2CPre<U>>(), MapId<U>{});
+        } else {
+          switch (f.kind) {
+            case T213_FN_C2R_PREROTATOR:
+              loc(OffOfCol<U, RotGather<U, RotC2RPre<U>>>{f.template as<RotGather<U, RotC2RPre<U>>>()}, MapId<U>{}, MapId<U>{});
+              break;
+            case T213_FN_C2R_POSTROTATOR:
+              loc(OffOfCol<U, RotGather<U, RotC2RPost<U>>>{f.template as<RotGather<U, RotC2RPost<U>>>()}, MapId<U>{}, MapId<U>{});
+              break;
+            case T213_FN_R2C_PREROTATOR:
+              loc(OffOfCol<U, RotGather<U, RotR2CPre<U>>>{f.template as<RotGather<U, RotR2CPre<U>>>()}, MapId<U>{}, MapId<U>{});
+              break;
+            case T213_FN_R2C_POSTROTATOR:
+              loc(OffOfCol<U, RotGather<U, RotR2CPost<U>>>{f.template as<RotGather<U, RotR2CPost<U>>>()}, MapId<U>{}, MapId<U>{});
+              break;
+            case T213_FN_C2R_FUSED_PREOP:
+              loc(OffOfCol<U, ColC2RFusedPre<U>>{f.template as<ColC2RFusedPre<U>>()}, MapId<U>{}, MapId<U>{});
+              break;
+            default:
+              loc(OffOfCol<U, ColR2CFusedPost<U>>{f.template as<ColR2CFusedPost<U>>()}, MapId<U>{}, MapId<U>{});
+              break;
+          }
+        }
+        return true;
+      }
       auto go = [&](auto tag) {
         using F = typename decltype(tag)::type;
         switch (P.eb * 100 + P.aw) {

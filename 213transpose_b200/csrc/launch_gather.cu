@@ -451,6 +451,11 @@ int launch_k(Kern kern, int64_t grid, int threads, int64_t smem, int K, cudaStre
 
 }  // namespace
 
+int col_local_form(const FnSpec &f, int64_t m) {
+  if (m <= 0 || !local_params_ok(f, m)) return 0;
+  return local_form(f.kind);
+}
+
 bool fits32(const FnSpec &f, int64_t m, int64_t n) {
   const int64_t lim = (int64_t)1 << 31;
   // generous common bound: every functor's intermediates are below about
