@@ -389,6 +389,7 @@ __device__ __noinline__ void bx_col(const BPass &P, int64_t u0, int64_t u1, unsi
     char *sbase;
     strip(u, j0, wd, sbase);
     const uint32_t wpr = wd.get(), nw = (uint32_t)m * wpr;
+#pragma unroll 4
     for (uint32_t t = threadIdx.x; t < nw; t += blockDim.x) {
       const uint32_t r = wd.div(t), w = t - r * wpr;
       typename PK::U pk;
@@ -472,6 +473,7 @@ __device__ __noinline__ void bx_col_local(const BPass &P, const Off off, const F
       for (U ob = (U)warp * 32; ob < m; ob += (U)nwarps * 32) {
         const U myo = ob + lane;
         const U myrow = myo < m ? G(myo) : 0;
+#pragma unroll 4
         for (uint32_t r = lr; r < 32; r += rpi) {
           const U row = __shfl_sync(0xffffffffu, myrow, r);
           const U o = ob + r;
@@ -542,6 +544,7 @@ __device__ __noinline__ void bx_row(const BPass &P, int64_t u0, int64_t u1, unsi
     Wd *g = reinterpret_cast<Wd *>(P.data + r0 * (int64_t)n * EB);
     const uint32_t nw = (uint32_t)nr * wpr;
     const uint64_t i_base = md.mod((uint64_t)r0);
+#pragma unroll 4
     for (uint32_t w = threadIdx.x; w < nw; w += blockDim.x) {
       const uint32_t rr = wd.div(w);
       const U j0 = (U)(w - rr * wpr) * PER;

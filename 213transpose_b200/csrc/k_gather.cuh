@@ -538,6 +538,7 @@ __global__ void __launch_bounds__(kGatherThreads)
       for (U sb = (U)warp * 32; sb < nslots; sb += (U)nwarps * 32) {
         const U mys = sb + lane;
         const U myrow = mys < nslots ? F(key_of_slot(mys)) : 0;
+#pragma unroll 4
         for (uint32_t r = lr; r < 32; r += rpi) {
           const U row = __shfl_sync(0xffffffffu, myrow, r);
           const U sl = sb + r;
@@ -560,6 +561,7 @@ __global__ void __launch_bounds__(kGatherThreads)
       for (U ob = (U)warp * 32; ob < nout; ob += (U)nwarps * 32) {
         const U myo = ob + lane;
         const U myrow = myo < nout ? G(k0 + myo) : 0;
+#pragma unroll 4
         for (uint32_t r = lr; r < 32; r += rpi) {
           const U row = __shfl_sync(0xffffffffu, myrow, r);
           const U o = ob + r;

@@ -311,6 +311,7 @@ double seg_eff(int64_t seg_bytes) {
 }
 
 std::string fmt_plan(const Plan &P) {
+  VariantScope vs(P.var);  // the pass descriptions show the kernels this plan's variant picks
   static const char *kn[] = {"auto", "c2r", "r2c", "skinny", "blocks", "bands", "bands_t", "identity", "slice"};
   std::string s = kn[P.kind >= 0 && P.kind <= 8 ? P.kind : 0];
   char buf[256];
@@ -663,6 +664,7 @@ std::shared_ptr<Plan> get_plan_variant(int64_t d1, int64_t d2, int64_t d3, int e
   }
   auto P = std::make_shared<Plan>(*base);
   P->var = v;
+  P->desc = fmt_plan(*P);  // the pass descriptions under this variant
   char buf[64];
   snprintf(buf, sizeof buf, " [variant col=%d row=%d tile=%d seg=%d]", v.col, v.row, v.tile, v.seg);
   P->desc += buf;
