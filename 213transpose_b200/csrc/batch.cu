@@ -81,6 +81,7 @@ int64_t direct_threshold() {
 int aw_for(int eb, const void *data, int64_t pitch) {
   if (eb >= 16) return 16;
   if (eb >= 4 && ((((uintptr_t)data) | (uint64_t)pitch) % 16 == 0)) return 16;
+  if (eb == 4 && ((((uintptr_t)data) | (uint64_t)pitch) % 8 == 0)) return 8;
   return eb;
 }
 

@@ -72,7 +72,7 @@ bool dispatch_eb_aw(int eb, int aw, Fn &&fn) {
     case 2:
       return fn(IC<2>{}, IC<2>{});
     case 4:
-      return aw == 16 ? fn(IC<4>{}, IC<16>{}) : fn(IC<4>{}, IC<4>{});
+      return aw == 16 ? fn(IC<4>{}, IC<16>{}) : aw == 8 ? fn(IC<4>{}, IC<8>{}) : fn(IC<4>{}, IC<4>{});
     case 8:
       return aw == 16 ? fn(IC<8>{}, IC<16>{}) : fn(IC<8>{}, IC<8>{});
     case 16:

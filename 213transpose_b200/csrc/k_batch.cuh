@@ -763,6 +763,7 @@ __device__ bool bx_dispatch(const BPass &P, const AnyFn<U> &f, int64_t u0, int64
             case 202: bx_col_local<2, 2, U, Off, Fm, Gm>(P, off, F, G, u0, u1, smem, s_sh); break;
             case 404: bx_col_local<4, 4, U, Off, Fm, Gm>(P, off, F, G, u0, u1, smem, s_sh); break;
             case 416: bx_col_local<4, 16, U, Off, Fm, Gm>(P, off, F, G, u0, u1, smem, s_sh); break;
+            case 408: bx_col_local<4, 8, U, Off, Fm, Gm>(P, off, F, G, u0, u1, smem, s_sh); break;
             case 808: bx_col_local<8, 8, U, Off, Fm, Gm>(P, off, F, G, u0, u1, smem, s_sh); break;
             case 816: bx_col_local<8, 16, U, Off, Fm, Gm>(P, off, F, G, u0, u1, smem, s_sh); break;
             default: bx_col_local<16, 16, U, Off, Fm, Gm>(P, off, F, G, u0, u1, smem, s_sh); break;
@@ -803,6 +804,7 @@ __device__ bool bx_dispatch(const BPass &P, const AnyFn<U> &f, int64_t u0, int64
           case 202: bx_col<2, 2, U, F>(P, u0, u1, smem); break;
           case 404: bx_col<4, 4, U, F>(P, u0, u1, smem); break;
           case 416: bx_col<4, 16, U, F>(P, u0, u1, smem); break;
+            case 408: bx_col<4, 8, U, F>(P, u0, u1, smem); break;
           case 808: bx_col<8, 8, U, F>(P, u0, u1, smem); break;
           case 816: bx_col<8, 16, U, F>(P, u0, u1, smem); break;
           default: bx_col<16, 16, U, F>(P, u0, u1, smem); break;
@@ -828,6 +830,7 @@ __device__ bool bx_dispatch(const BPass &P, const AnyFn<U> &f, int64_t u0, int64
           case 202: bx_row<2, 2, U, F>(P, u0, u1, smem); break;
           case 404: bx_row<4, 4, U, F>(P, u0, u1, smem); break;
           case 416: bx_row<4, 16, U, F>(P, u0, u1, smem); break;
+            case 408: bx_row<4, 8, U, F>(P, u0, u1, smem); break;
           case 808: bx_row<8, 8, U, F>(P, u0, u1, smem); break;
           case 816: bx_row<8, 16, U, F>(P, u0, u1, smem); break;
           default: bx_row<16, 16, U, F>(P, u0, u1, smem); break;

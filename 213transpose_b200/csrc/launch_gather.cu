@@ -62,9 +62,18 @@ int aligned16(const void *p, int64_t pitch_bytes) {
   return (((uintptr_t)p | (uint64_t)pitch_bytes) & 15) == 0;
 }
 
+// Access word of the gather kernels: 16 bytes when the base and the pitch
+// allow, 8 bytes for 4-byte elements on an 8-byte pitch (half the
+// instructions of 4-byte words), else the element.  T213_AW_MAX (4, 8 or 16)
+// caps it, for measuring the widths against each other.
 int pick_aw(int eb, const void *data, int64_t pitch_bytes, int64_t extra_bytes) {
   if (eb >= 16) return 16;
-  if (eb >= 4 && aligned16(data, pitch_bytes) && (extra_bytes & 15) == 0) return 16;
+  static const int cap = [] {
+    const char *v = std::getenv("T213_AW_MAX");
+    return v && std::atoi(v) > 0 ? std::atoi(v) : 16;
+  }();
+  if (eb >= 4 && cap >= 16 && aligned16(data, pitch_bytes) && (extra_bytes & 15) == 0) return 16;
+  if (eb == 4 && cap >= 8 && ((((uintptr_t)data | (uint64_t)pitch_bytes | (uint64_t)extra_bytes) & 7) == 0)) return 8;
   return eb;
 }
 
