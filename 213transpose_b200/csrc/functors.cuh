@@ -183,43 +183,79 @@ struct RowR2CShuffle {  // equations.h:178-194
   }
 };
 
-// Row shufflers evaluated along a row, at (i, j), (i, j + 1), ...: when m and
-// n are coprime both shuffles step by a constant modulo n (C2R: s = k (j - i)
-// mod n grows by k; R2C: s = (i + j m) mod n grows by m mod n), so the next
-// value is an add and a conditional subtract.  Other row functors, and the
-// shuffles of non-coprime shapes, are evaluated anew.
+// Row shufflers evaluated along a row: first(i, j), then next(i, j + 1),
+// next(i, j + 2), ... carry the functor's intermediate values from one column
+// to the next.  Any other row functor is evaluated anew at every column.
 template <typename F, typename U>
 struct RowStepper {
   const F &f;
   T213_HD explicit RowStepper(const F &f_) : f(f_) {}
-  T213_HD U next(U, U i, U j) const { return f(i, j); }
+  T213_HD U first(U i, U j) { return f(i, j); }
+  T213_HD U next(U i, U j) { return f(i, j); }
 };
 
+// C2R shuffle.  Coprime m, n: s = k (j - i) mod n grows by k.  Otherwise, with
+// jc = j mod c, f = j + i (n - 1) (+ m when i - jc > m - c), q = f / c, r =
+// f mod c and s = (k (q mod b)) mod b + r b: while the +m term stays put, f
+// grows by one, so r does, carrying into q, whose term (k q) mod b then grows
+// by k mod b; when the +m term flips (jc wrapping, or reaching the bound),
+// everything is evaluated anew.
 template <typename U>
 struct RowStepper<RowC2RShuffle<U>, U> {
   const RowC2RShuffle<U> &f;
-  U inc, n;
-  bool on;
+  U n, b, c, k, i = 0, jc = 0, rem = 0, bq = 0, kb = 0, s = 0;
+  bool low = false;
   T213_HD explicit RowStepper(const RowC2RShuffle<U> &f_)
-      : f(f_), inc(f_.k), n(f_.n.get()), on(f_.c.get() == 1) {}
-  T213_HD U next(U s, U i, U j) const {
-    if (!on) return f(i, j);
-    const U t = s + inc;
-    return t >= n ? t - n : t;
+      : f(f_), n(f_.n.get()), b(f_.b.get()), c(f_.c.get()), k(f_.k) {}
+  T213_HD U first(U i_, U j) {
+    if (c == 1) return s = f(i_, j);
+    i = i_;
+    jc = f.c.mod(j);
+    low = i + c <= f.m + jc;
+    const U ff = j + i * (n - 1) + (low ? 0 : f.m);
+    const U qq = f.c.div(ff);
+    rem = ff - qq * c;
+    bq = f.b.mod(qq);
+    kb = f.b.mod(k * bq);
+    return s = kb + rem * b;
+  }
+  T213_HD U next(U i_, U j) {
+    if (c == 1) {
+      const U t = s + k;
+      return s = t >= n ? t - n : t;
+    }
+    if (++jc == c) jc = 0;
+    if ((i + c <= f.m + jc) != low) return first(i_, j);
+    if (++rem == c) {
+      rem = 0;
+      if (++bq == b) bq = 0;
+      kb += k;
+      if (kb >= b) kb -= b;
+    }
+    return s = kb + rem * b;
   }
 };
 
+// R2C shuffle: s = ((j / b + i) mod m + j m) mod n grows by m mod n while j / b
+// stays put (always, when m and n are coprime: b = n); at a multiple of b it
+// is evaluated anew.
 template <typename U>
 struct RowStepper<RowR2CShuffle<U>, U> {
   const RowR2CShuffle<U> &f;
-  U inc, n;
-  bool on;
+  U inc, n, b, jb = 0, s = 0;
   T213_HD explicit RowStepper(const RowR2CShuffle<U> &f_)
-      : f(f_), inc(f_.n.mod(f_.m.get())), n(f_.n.get()), on(f_.b.get() == f_.n.get()) {}
-  T213_HD U next(U s, U i, U j) const {
-    if (!on) return f(i, j);
+      : f(f_), inc(f_.n.mod(f_.m.get())), n(f_.n.get()), b(f_.b.get()) {}
+  T213_HD U first(U i, U j) {
+    jb = b == n ? 0 : f.b.mod(j);
+    return s = f(i, j);
+  }
+  T213_HD U next(U i, U j) {
+    if (b != n && ++jb == b) {
+      jb = 0;
+      return s = f(i, j);
+    }
     const U t = s + inc;
-    return t >= n ? t - n : t;
+    return s = t >= n ? t - n : t;
   }
 };
 

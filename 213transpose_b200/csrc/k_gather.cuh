@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(kGatherThreads)
     const U qh = (U)((c0 - b0) / EB), qt = (U)((c1 - b0) / EB);
     const uint32_t nvec = (uint32_t)((c1 - c0) >> 4);
     uint4 *gout = reinterpret_cast<uint4 *>(c0);
-    const RowStepper<F, U> step(fn);
+    RowStepper<F, U> step(fn);
     for (uint32_t v = threadIdx.x; v < nvec; v += blockDim.x) {
       U rr, j, i;
       locate(qh + (U)v * PER, rr, j, i);
@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(kGatherThreads)
         uint4 w;
         E e[PER];
       } pk;
-      U s = fn(i, j);
+      U s = step.first(i, j);
 #pragma unroll
       for (int e = 0; e < PER; e++) {
         if (e > 0) {
@@ -186,9 +186,9 @@ __global__ void __launch_bounds__(kGatherThreads)
             j = 0;
             rr++;
             if (++i == m) i = 0;
-            s = fn(i, j);
+            s = step.first(i, j);
           } else {
-            s = step.next(s, i, j);
+            s = step.next(i, j);
           }
         }
         pk.e[e] = sm[d0 + rr * n + s];
