@@ -295,7 +295,12 @@ int build_batch_tables(const t213_tensor_desc *tensors, int32_t count, const std
           bp.aw = aw_for(eb, data, q.n * eb);
           bp.rows_per_unit = std::max<int64_t>(1, std::min<int64_t>(q.m, (64 * 1024) / std::max<int64_t>(1, q.n * eb)));
           bp.n_units = (d.d3 * q.m + bp.rows_per_unit - 1) / bp.rows_per_unit;
-          bp.div_w = FastDiv<uint32_t>((uint64_t)(q.n / (bp.aw / eb)));
+          // elements of at most 4 bytes on a pitch that is not a 16-byte
+          // multiple: the peeled executor (16-byte words, stepped shuffles);
+          // its divisor is then n itself
+          bp.row_peel = bp.aw < 16 && eb <= 4 && std::getenv("T213_BATCH_ROW_WORDS") == nullptr &&
+                        q.n * eb * bp.rows_per_unit + 32 <= kBatchHalf;
+          bp.div_w = FastDiv<uint32_t>((uint64_t)(bp.row_peel ? q.n : q.n / (bp.aw / eb)));
           bp.div_m = FastDiv<uint64_t>((uint64_t)q.m);
           bp.u64 = !fits32(q.fn, q.m, q.n);
           if (bp.u64)

@@ -106,6 +106,7 @@ struct BPass {
   int64_t t = 0, Bm = 0, Bn = 0, nt = 0, pairs = 0;  // TILE
   int32_t tile_vec = 0, band_vec = 0;
   int32_t col_form = 0;                    // COL: cluster-local form 1-3 of the functor, 0 = evaluate it per element
+  int32_t row_peel = 0;                    // ROW: 16-byte accesses over a pitch that is not a 16-byte multiple
   int64_t R = 0, C = 0;                    // BAND
   const Chunk *chunks = nullptr;           // SEG / CARRY
   const CarryItem *carries = nullptr;
@@ -551,9 +552,102 @@ __device__ __noinline__ void bx_row(const BPass &P, int64_t u0, int64_t u1, unsi
       const uint64_t ii = i_base + rr;
       const U i = (U)(ii < (uint64_t)m ? ii : md.mod(ii));
       typename PK::U pk;
+      RowStepper<F, U> step(fn);
 #pragma unroll
-      for (int e = 0; e < PER; e++) pk.e[e] = sm[(int64_t)rr * n + fn(i, j0 + e)];
+      for (int e = 0; e < PER; e++)
+        pk.e[e] = sm[(int64_t)rr * n + (e == 0 ? step.first(i, j0) : step.next(i, j0 + e))];
       __stcs(g + w, pk.w);
+    }
+    __syncthreads();
+  }
+}
+
+// ROW items whose pitch is not a 16-byte multiple, for elements of at most 4
+// bytes: the unit (consecutive rows, one contiguous byte range [b0, b1)) is
+// staged as the 16-byte blocks that cover it (bytes of the neighbouring units
+// at both ends are read and never used) and written back with 16-byte stores
+// between its first and last 16-byte boundary, single elements at the ends.
+// A thread takes 16/EB consecutive elements and steps the shuffle along them.
+template <int EB, typename U, typename F>
+__device__ __noinline__ void bx_row_peel(const BPass &P, int64_t u0, int64_t u1, unsigned char *smem) {
+  using E = typename ElemT<EB>::type;
+  constexpr int PER = 16 / EB;
+  const F fn = any_fn<U>(P).template as<F>();
+  const U m = (U)P.m, n = (U)P.n;
+  const FastDiv<uint32_t> nd = P.div_w;  // n (elements per row)
+  const FastDiv<uint64_t> md = P.div_m;  // m
+  const int64_t total_rows = P.d3 * P.m, row_bytes = P.n * EB;
+  auto range = [&](int64_t u, uintptr_t &b0, uintptr_t &b1) {
+    const int64_t r0 = u * P.rows_per_unit;
+    const int64_t nr = min((int64_t)P.rows_per_unit, total_rows - r0);
+    b0 = reinterpret_cast<uintptr_t>(P.data + r0 * row_bytes);
+    b1 = b0 + (uintptr_t)(nr * row_bytes);
+  };
+  auto stage = [&](int64_t u, unsigned char *buf) {
+    uintptr_t b0, b1;
+    range(u, b0, b1);
+    const uintptr_t a0 = b0 & ~(uintptr_t)15, a1 = (b1 + 15) & ~(uintptr_t)15;
+    const uint32_t nv = (uint32_t)((a1 - a0) >> 4);
+    const uint4 *g = reinterpret_cast<const uint4 *>(a0);
+    for (uint32_t v = threadIdx.x; v < nv; v += blockDim.x) cp_async<16>(buf + 16 * (size_t)v, g + v);
+    cp_async_commit();
+  };
+  stage(u0, smem);
+  for (int64_t u = u0; u < u1; u++) {
+    const E *sm = reinterpret_cast<const E *>(smem + ((u - u0) & 1) * kBatchHalf);
+    if (u + 1 < u1) {
+      stage(u + 1, smem + ((u + 1 - u0) & 1) * kBatchHalf);
+      cp_async_wait_group<1>();
+    } else {
+      cp_async_wait_group<0>();
+    }
+    __syncthreads();
+    uintptr_t b0, b1;
+    range(u, b0, b1);
+    const int64_t r0 = u * P.rows_per_unit;
+    const U d0 = (U)((b0 - (b0 & ~(uintptr_t)15)) / EB);  // unit element 0 sits at sm[d0]
+    const U i_base = (U)md.mod((uint64_t)r0);
+    const U total = (U)((b1 - b0) / EB);
+    auto locate = [&](U q, U &rr, U &j, U &i) {
+      rr = (U)nd.div((uint32_t)q);
+      j = q - rr * n;
+      const uint64_t ii = (uint64_t)i_base + rr;
+      i = (U)(ii < (uint64_t)m ? ii : md.mod(ii));
+    };
+    const uintptr_t c0 = min((b0 + 15) & ~(uintptr_t)15, b1), c1 = max(b1 & ~(uintptr_t)15, c0);
+    const U qh = (U)((c0 - b0) / EB), qt = (U)((c1 - b0) / EB);
+    const uint32_t nvec = (uint32_t)((c1 - c0) >> 4);
+    uint4 *gout = reinterpret_cast<uint4 *>(c0);
+    RowStepper<F, U> step(fn);
+    for (uint32_t v = threadIdx.x; v < nvec; v += blockDim.x) {
+      U rr, j, i;
+      locate(qh + (U)v * PER, rr, j, i);
+      union {
+        uint4 w;
+        E e[PER];
+      } pk;
+      U s = step.first(i, j);
+#pragma unroll
+      for (int e = 0; e < PER; e++) {
+        if (e > 0) {
+          if (++j == n) {
+            j = 0;
+            rr++;
+            if (++i == m) i = 0;
+            s = step.first(i, j);
+          } else {
+            s = step.next(i, j);
+          }
+        }
+        pk.e[e] = sm[d0 + rr * n + s];
+      }
+      __stcs(gout + v, pk.w);
+    }
+    for (U t = threadIdx.x; t < qh + (total - qt); t += blockDim.x) {
+      const U q = t < qh ? t : qt + (t - qh);
+      U rr, j, i;
+      locate(q, rr, j, i);
+      reinterpret_cast<E *>(b0)[q] = sm[d0 + rr * n + fn(i, j)];
     }
     __syncthreads();
   }
@@ -836,6 +930,21 @@ __device__ bool bx_dispatch(const BPass &P, const AnyFn<U> &f, int64_t u0, int64
           default: bx_row<16, 16, U, F>(P, u0, u1, smem); break;
         }
       };
+      if (P.row_peel) {
+        auto gp = [&](auto tag) {
+          using F = typename decltype(tag)::type;
+          switch (P.eb) {
+            case 1: bx_row_peel<1, U, F>(P, u0, u1, smem); break;
+            case 2: bx_row_peel<2, U, F>(P, u0, u1, smem); break;
+            default: bx_row_peel<4, U, F>(P, u0, u1, smem); break;
+          }
+        };
+        if (f.kind == T213_FN_R2C_SHUFFLE)
+          gp(TypeTag<RowR2CShuffle<U>>{});
+        else
+          gp(TypeTag<RowC2RShuffle<U>>{});
+        return true;
+      }
       if (f.kind == T213_FN_R2C_SHUFFLE)
         go(TypeTag<RowR2CShuffle<U>>{});
       else
