@@ -108,7 +108,9 @@ struct LaunchStats {
 // per shape class.
 struct Variant {
   int8_t col = 0;   // column passes: 1 staged strips (no cluster-local form), 2 cluster-local 256-byte strips,
-                    // 3 cluster-local double-buffered, 4 the same with half-size buffers (two CTAs per SM)
+                    // 3 cluster-local double-buffered, 4 the same with half-size buffers (two CTAs per SM),
+                    // 5 word-width cluster-local strips where the default takes 16-byte accesses over an
+                    // unaligned pitch (k_col_local_peel)
   int8_t row = 0;   // row passes: 1 staged rows, 2 double-buffered rows (k_row_pipe), 3 word-width staged rows
                     // where the default takes 16-byte accesses over an unaligned pitch (k_row_gather_peel)
   int8_t tile = 0;  // tile swaps: 1 TMA ring, 2 register tiles (k_tile_swap_vec)

@@ -607,6 +607,207 @@ __global__ void __launch_bounds__(kGatherThreads)
   }
 }
 
+// ---------------------------------------------------------------------------
+// k_col_local with 16-byte global accesses for rows whose pitch is not a
+// multiple of 16 bytes (4- and 8-byte elements, n odd or n = 2 mod 4).  A strip
+// is W * EB = 16 L bytes wide, so its start has the same offset a(row) inside
+// a 16-byte block as its row (the strip starts are 16-byte multiples apart).
+// A slot of shared memory (stride SB = 16 L + 16 bytes) takes the 16-byte
+// blocks covering the strip's bytes of one source row: L of them, or L + 1
+// when a(row) != 0; up to 15 bytes on either side belong to the neighbouring
+// strips and are read and never used.  Element q of the slot sits at byte
+// a + q * EB; a per-slot byte table keeps a.  An output row is written by L
+// lanes: lane l takes the 16-byte block that starts h + l * PER elements into
+// the row (h = elements before the row's first 16-byte boundary), so every
+// lane but the last stores one 16-byte vector; the last lane's block runs
+// past the strip by h elements, which are the row's first h elements: it
+// stores its elements one by one, those past the strip at the row's start.
+// The last strip of a row, when narrower, moves element by element.
+// Cluster, halo and key-space logic are those of k_col_local.
+// ---------------------------------------------------------------------------
+template <int EB, typename U, typename Off, typename Fsrc, typename Gout, bool CLUSTER>
+__global__ void __launch_bounds__(kGatherThreads)
+    k_col_local_peel(char *__restrict__ data, int64_t d3, U m, U n, U W, U SB, U max_slots, int64_t n_strips, U H,
+                     int halo, Off off, Fsrc F, Gout G, int *status) {
+  static_assert(EB == 4 || EB == 8, "4- and 8-byte elements");
+  using E = typename ElemT<EB>::type;
+  constexpr int PER = 16 / EB;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned char *s_al = smem_raw + (size_t)max_slots * SB;  // per slot: byte offset of element 0
+  __shared__ int s_sh[256];
+  __shared__ int s_span;
+  __shared__ U s_base;
+
+  int rank = 0, K = 1;
+  int64_t unit0 = blockIdx.x, ustride = gridDim.x;
+  if (CLUSTER) {
+    cg::cluster_group cl = cg::this_cluster();
+    rank = (int)cl.block_rank();
+    K = (int)cl.num_blocks();
+    unit0 = blockIdx.x / K;
+    ustride = gridDim.x / K;
+  }
+  const bool whole = !CLUSTER && H >= m;
+  const int64_t n_units = d3 * n_strips;
+  const U k0 = (U)min((int64_t)rank * (int64_t)H, (int64_t)m);
+  const U k1 = (U)min((int64_t)k0 + (int64_t)H, (int64_t)m);
+  const U nk = k1 - k0;
+  const int64_t pitch = (int64_t)n * EB;
+  const uint32_t pm = (uint32_t)(pitch & 15);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const uint32_t L = (uint32_t)(W * EB / 16);  // lanes per row; divides 32 (host: W * EB in {64, 128, 256})
+  const uint32_t rpi = 32 / L, lr = lane / L, lw = lane - lr * L;
+
+  for (int64_t u = unit0; u < n_units; u += ustride) {
+    const int64_t k = u / n_strips;
+    const U s = (U)(u - k * n_strips);
+    const U j0 = s * W;
+    const U wn = min(W, n - j0);
+    char *sbase = data + (k * (int64_t)m * n + j0) * EB;
+    // offset of the strip inside a 16-byte block: (cb + row * pm) & 15
+    const uint32_t cb = (uint32_t)(reinterpret_cast<uintptr_t>(sbase) & 15);
+    if (warp == 0) {
+      const int64_t mm = (int64_t)m;
+      const int64_t r0 = (int64_t)off(j0);
+      int dmin = 0, dmax = 0;
+      for (U w = lane; w < wn; w += 32) {
+        const int64_t rw = (int64_t)off(j0 + w);
+        int64_t d = rw - r0;
+        if (2 * d > mm) d -= mm;
+        if (2 * d <= -mm) d += mm;
+        s_sh[w] = whole ? (int)rw : (int)d;
+        dmin = min(dmin, (int)d);
+        dmax = max(dmax, (int)d);
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        dmin = min(dmin, __shfl_xor_sync(0xffffffffu, dmin, o));
+        dmax = max(dmax, __shfl_xor_sync(0xffffffffu, dmax, o));
+      }
+      __syncwarp();
+      if (!whole)
+        for (U w = lane; w < wn; w += 32) s_sh[w] -= dmin;
+      if (lane == 0) {
+        s_span = whole ? 0 : dmax - dmin;
+        int64_t b = whole ? 0 : ((int64_t)k0 + r0 + dmin) % mm;
+        if (b < 0) b += mm;
+        s_base = (U)b;
+      }
+    }
+    __syncthreads();
+    const bool fits = s_span <= halo;
+    if (!fits && threadIdx.x == 0) atomicExch(status, 1 /* T213_ERR_INVALID_ARGUMENT */);
+    const U nslots = !fits ? 0 : whole ? m : (nk > 0 ? nk + (U)s_span : 0);
+    const U nout = fits ? nk : 0;
+    const U base = s_base;
+    auto key_of_slot = [&](U sl) -> U {
+      U key = base + sl;
+      return key >= m ? key - m : key;
+    };
+    auto slot_of = [&](U o, int sh) -> U {
+      if (whole) {
+        U v = k0 + o + (U)sh;
+        return v >= m ? v - m : v;
+      }
+      return o + (U)sh;
+    };
+    auto elem = [&](U sl, U q) -> E {
+      return *reinterpret_cast<const E *>(smem_raw + (size_t)sl * SB + s_al[sl] + (size_t)q * EB);
+    };
+    if (wn == W) {
+      // ---- loads: L lanes per source row, one more block when unaligned ----
+      for (U sb = (U)warp * 32; sb < nslots; sb += (U)nwarps * 32) {
+        const U mys = sb + lane;
+        const U myrow = mys < nslots ? F(key_of_slot(mys)) : 0;
+        if (mys < nslots) s_al[mys] = (unsigned char)((cb + (uint32_t)myrow * pm) & 15u);
+#pragma unroll 4
+        for (uint32_t r = lr; r < 32; r += rpi) {
+          const U row = __shfl_sync(0xffffffffu, myrow, r);
+          const U sl = sb + r;
+          if (sl < nslots) {
+            const uintptr_t A = reinterpret_cast<uintptr_t>(sbase + (int64_t)row * pitch);
+            const char *g0 = reinterpret_cast<const char *>(A & ~(uintptr_t)15);
+            unsigned char *d0 = smem_raw + (size_t)sl * SB;
+            cp_async<16>(d0 + 16 * lw, g0 + 16 * lw);
+            if (lw == L - 1 && (A & 15)) cp_async<16>(d0 + 16 * L, g0 + 16 * L);
+          }
+        }
+      }
+      cp_async_wait_all();
+      if (CLUSTER)
+        cg::this_cluster().sync();
+      else
+        __syncthreads();
+      // ---- stores: the shifts of the 2 PER - 1 columns a lane may take -----
+      int shr[2 * PER - 1];
+#pragma unroll
+      for (int t = 0; t < 2 * PER - 1; t++) {
+        uint32_t q = lw * PER + t;
+        if (q >= (uint32_t)W) q -= (uint32_t)W;
+        shr[t] = s_sh[q];
+      }
+      for (U ob = (U)warp * 32; ob < nout; ob += (U)nwarps * 32) {
+        const U myo = ob + lane;
+        const U myrow = myo < nout ? G(k0 + myo) : 0;
+#pragma unroll 2
+        for (uint32_t r = lr; r < 32; r += rpi) {
+          const U row = __shfl_sync(0xffffffffu, myrow, r);
+          const U o = ob + r;
+          if (o < nout) {
+            char *B = sbase + (int64_t)row * pitch;
+            const uint32_t ab = (cb + (uint32_t)row * pm) & 15u;
+            const uint32_t h = ((16u - ab) & 15u) / EB;  // elements before the row's first 16-byte boundary
+            union {
+              uint4 w;
+              E e[PER];
+            } pk;
+#pragma unroll
+            for (int e = 0; e < PER; e++) {
+              int sh = shr[e];
+#pragma unroll
+              for (int t = 1; t < PER; t++)
+                if (h == (uint32_t)t) sh = shr[t + e];
+              U q = (U)(lw * PER + h + e);
+              if (q >= W) q -= W;
+              pk.e[e] = elem(slot_of(o, sh), q);
+            }
+            if (lw < L - 1 || h == 0) {
+              __stcs(reinterpret_cast<uint4 *>(B + (size_t)(h + lw * PER) * EB), pk.w);
+            } else {
+#pragma unroll
+              for (int e = 0; e < PER; e++) {
+                U q = (U)(lw * PER + h + e);
+                if (q >= W) q -= W;
+                reinterpret_cast<E *>(B)[q] = pk.e[e];
+              }
+            }
+          }
+        }
+      }
+    } else {
+      // ---- the narrower last strip: element by element, element q at q * EB --
+      const uint32_t nw = (uint32_t)nslots * (uint32_t)wn;
+      for (uint32_t t = threadIdx.x; t < nw; t += blockDim.x) {
+        const uint32_t sl = t / (uint32_t)wn, q = t - sl * (uint32_t)wn;
+        const U row = F(key_of_slot((U)sl));
+        if (q == 0) s_al[sl] = 0;
+        cp_async<EB>(smem_raw + (size_t)sl * SB + (size_t)q * EB, sbase + (int64_t)row * pitch + (int64_t)q * EB);
+      }
+      cp_async_wait_all();
+      if (CLUSTER)
+        cg::this_cluster().sync();
+      else
+        __syncthreads();
+      const uint32_t nwo = (uint32_t)nout * (uint32_t)wn;
+      for (uint32_t t = threadIdx.x; t < nwo; t += blockDim.x) {
+        const uint32_t o = t / (uint32_t)wn, q = t - o * (uint32_t)wn;
+        const U row = G(k0 + (U)o);
+        reinterpret_cast<E *>(sbase + (int64_t)row * pitch)[q] = elem(slot_of((U)o, s_sh[q]), (U)q);
+      }
+    }
+    __syncthreads();  // shared memory, the slot table and s_sh are reused by the next strip
+  }
+}
+
 // Double-buffered form of k_col_local: shared memory holds two strips, and
 // the loads of a CTA's next strip are issued right after the barrier that
 // ends the current strip's loads, so they are in flight while the current

@@ -190,6 +190,10 @@ struct LocalCfg {
   int64_t W = 0, WS = 0, H = 0, halo = 0, smem = 0;  // smem: one strip buffer
   bool u64 = false;
   bool db = false;  // double-buffered kernel (two strip buffers)
+  // k_col_local_peel: 16-byte accesses although the pitch is not a 16-byte
+  // multiple; SB = slot stride in bytes, max_slots = slots of one strip buffer
+  bool peel = false;
+  int64_t SB = 0, max_slots = 0;
 };
 
 // Largest (dmax - dmin) over the strips of width W: the key offsets of one
@@ -295,6 +299,66 @@ LocalCfg local_col_config(const FnSpec &f, int64_t m, int64_t n, int eb, const v
   const int64_t buf_cap = dbmode ? kSmemCap / 2 - 64 : kSmemCap;
   const int64_t whole_cap =
       std::min<int64_t>(buf_cap, (env_int("T213_COL_WHOLE_KB") > 0 ? env_int("T213_COL_WHOLE_KB") : 104) * 1024);
+  // narrow access words for 4- and 8-byte elements (the pitch or the base is
+  // not 16-byte aligned): the peeled kernel moves the same strips with
+  // 16-byte accesses (variant col=5 or T213_COL_PEEL=0 keep the word-width
+  // kernel)
+  const char *pe = std::getenv("T213_COL_PEEL");
+  if ((eb == 4 || eb == 8) && c.aw < 16 && (reinterpret_cast<uintptr_t>(data) % (uintptr_t)eb) == 0 && !dbmode &&
+      pv.col != 5 && !(pe && std::atoi(pe) == 0)) {
+    c.peel = true;
+    c.aw = 16;
+    auto slot_bytes = [](int64_t wb) { return wb + 16 + 1; };  // blocks of a slot + its byte in the offset table
+    if (m * slot_bytes(128) <= whole_cap && env_int("T213_COL_LOCAL_K") <= 1 && pv.col != 2) {
+      int64_t wb = 128;
+      const int64_t target = std::max<int64_t>(128, (48 * 1024) / m);
+      while (2 * wb <= 512 && 2 * wb <= target && 2 * wb <= round_up(n * eb, 16)) wb *= 2;
+      while (wb > 128 && m * slot_bytes(wb) > whole_cap) wb /= 2;
+      c.W = wb / eb;
+      c.WS = c.W;
+      c.SB = wb + 16;
+      c.K = 1;
+      c.H = m;
+      c.halo = 0;
+      c.max_slots = m;
+      c.smem = m * c.SB + round_up(m, 16);
+      c.ok = true;
+      return c;
+    }
+    struct Try {
+      int64_t wbytes, kb;
+    };
+    std::vector<Try> tries;
+    if (env_int("T213_COL_LOCAL_WBYTES") >= 64 || env_int("T213_COL_LOCAL_SMEM_KB") > 0)
+      tries.push_back({env_int("T213_COL_LOCAL_WBYTES") >= 64 ? env_int("T213_COL_LOCAL_WBYTES") : 128,
+                       env_int("T213_COL_LOCAL_SMEM_KB") > 0 ? env_int("T213_COL_LOCAL_SMEM_KB") : 100});
+    else if (pv.col == 2)
+      tries = {{256, 110}, {256, 200}, {128, 100}, {128, 200}, {64, 200}};
+    else
+      tries = {{128, 100}, {128, 200}, {64, 200}};
+    for (const Try &t : tries) {
+      if (t.wbytes != 64 && t.wbytes != 128 && t.wbytes != 256 && t.wbytes != 512) continue;
+      c.W = t.wbytes / eb;
+      c.WS = c.W;
+      c.SB = t.wbytes + 16;
+      c.halo = local_span(f, m, n, c.W);
+      if (c.halo > kColHaloMax) continue;
+      const int64_t hmax = std::max<int64_t>(1, (t.kb * 1024) / slot_bytes(t.wbytes) - c.halo);
+      c.K = (int)std::min<int64_t>(kMaxCluster + 1, (m + hmax - 1) / hmax);
+      if (env_int("T213_COL_LOCAL_K") > 1) c.K = env_int("T213_COL_LOCAL_K");
+      if (c.K > kMaxCluster || c.K < 2) continue;
+      c.H = (m + c.K - 1) / c.K;
+      c.max_slots = c.H + c.halo;
+      c.smem = c.max_slots * c.SB + round_up(c.max_slots, 16);
+      if (c.smem > buf_cap) continue;
+      c.ok = true;
+      return c;
+    }
+    // no peeled strip fits: the word-width kernel below
+    c.peel = false;
+    c.aw = pick_aw(eb, data, n * eb, 0);
+    c.SB = c.max_slots = 0;
+  }
   if (m * 128 <= whole_cap && env_int("T213_COL_LOCAL_K") <= 1 && pv.col != 2) {
     // whole strips in one CTA: at least 128-byte rows, widened to about
     // 48 KB per strip (at most 256 columns), no halo
@@ -506,8 +570,9 @@ std::string describe_col_gather_fn(const FnSpec &f, int64_t m, int64_t n, int eb
   LocalCfg lc = local_col_config(f, m, n, eb, data);
   if (lc.ok) {
     char buf[160];
-    snprintf(buf, sizeof buf, "col_gather[local%s W=%lld cluster=%d halo=%lld smem=%lldK aw=%d]", lc.db ? " db" : "",
-             (long long)lc.W, lc.K, (long long)lc.halo, (long long)((lc.db ? 2 : 1) * lc.smem / 1024), lc.aw);
+    snprintf(buf, sizeof buf, "col_gather[local%s W=%lld cluster=%d halo=%lld smem=%lldK aw=%d%s]",
+             lc.db ? " db" : "", (long long)lc.W, lc.K, (long long)lc.halo,
+             (long long)((lc.db ? 2 : 1) * lc.smem / 1024), lc.aw, lc.peel ? " peeled" : "");
     return buf;
   }
   return describe_col_gather(m, n, eb, data);
@@ -568,6 +633,32 @@ int clusters_resident(const void *kern, int threads, int64_t smem, int K) {
   return v;
 }
 
+// Calls go(off, F, G) with the key offsets and the row maps of the functor's
+// cluster-local form (local_form).
+template <typename U, typename Go>
+void with_local_maps(const FnSpec &f, int64_t m, Go &&go) {
+  const int form = local_form(f.kind);
+  if (form == 1) {
+    with_col_fn<U>(f, m, [&](auto fn) -> bool {
+      go(OffOfCol<U, decltype(fn)>{fn}, MapId<U>{}, MapId<U>{});
+      return true;
+    });
+  } else if (form == 2) {  // p = {m, n', c}
+    const int64_t cc = f.p[2] > 0 ? f.p[2] : 1, a = m / cc, b = f.p[1] / cc;
+    int64_t binv = 0;
+    if (a > 1) {
+      ext_gcd(b % a, a, &binv);
+      binv %= a;
+      if (binv < 0) binv += a;
+    }
+    go(OffAffine<U, false>{FastDiv<U>((uint64_t)m)}, MapId<U>{}, PermR2CPre<U>(m, cc, binv));
+  } else {  // form 3, p = {a, c, m, q}
+    const int64_t cc = f.p[1] > 0 ? f.p[1] : 1, a = f.p[0] > 0 ? f.p[0] : 1;
+    const int64_t q = ((f.p[3] % a) + a) % a;
+    go(OffAffine<U, true>{FastDiv<U>((uint64_t)m)}, PermR2CPre<U>(m, cc, q), MapId<U>{});
+  }
+}
+
 // k_col_local for one element size / access width / index width.
 template <int EB, int AW, typename U>
 int launch_col_local_t(const FnSpec &f, const LocalCfg &c, char *data, int64_t d3, int64_t m, int64_t n,
@@ -622,26 +713,42 @@ int launch_col_local_t(const FnSpec &f, const LocalCfg &c, char *data, int64_t d
                         n_strips, (U)c.H, (int)c.halo, off, F, G, stw);
     }
   };
-  const int form = local_form(f.kind);
-  if (form == 1) {
-    with_col_fn<U>(f, m, [&](auto fn) -> bool {
-      go(OffOfCol<U, decltype(fn)>{fn}, MapId<U>{}, MapId<U>{});
-      return true;
-    });
-  } else if (form == 2) {  // p = {m, n', c}
-    const int64_t cc = f.p[2] > 0 ? f.p[2] : 1, a = m / cc, b = f.p[1] / cc;
-    int64_t binv = 0;
-    if (a > 1) {
-      ext_gcd(b % a, a, &binv);
-      binv %= a;
-      if (binv < 0) binv += a;
+  with_local_maps<U>(f, m, go);
+  return status;
+}
+
+// k_col_local_peel for one element size / index width.
+template <int EB, typename U>
+int launch_col_peel_t(const FnSpec &f, const LocalCfg &c, char *data, int64_t d3, int64_t m, int64_t n,
+                      cudaStream_t st) {
+  const int64_t n_strips = (n + c.W - 1) / c.W;
+  const int64_t units = n_strips * d3;
+  int status = T213_OK;
+  auto go = [&](auto off, auto F, auto G) {
+    using Off = decltype(off);
+    using Fs = decltype(F);
+    using Gs = decltype(G);
+    int *stw = device_status_word(&status);
+    if (!stw) return;
+    if (c.K == 1) {
+      auto kern = k_col_local_peel<EB, U, Off, Fs, Gs, false>;
+      if ((status = prep_kernel(kern, c.smem, 1))) return;
+      const int64_t grid = persistent_grid(kern, kGatherThreads, c.smem, 1, units);
+      status = launch_k(kern, grid, kGatherThreads, c.smem, 1, st, data, d3, (U)m, (U)n, (U)c.W, (U)c.SB,
+                        (U)c.max_slots, n_strips, (U)c.H, (int)c.halo, off, F, G, stw);
+    } else {
+      auto kern = k_col_local_peel<EB, U, Off, Fs, Gs, true>;
+      if ((status = prep_kernel(kern, c.smem, c.K))) return;
+      if (clusters_resident((const void *)kern, kGatherThreads, c.smem, c.K) < 1) {
+        status = kNoCluster;
+        return;
+      }
+      const int64_t grid = persistent_grid(kern, kGatherThreads, c.smem, c.K, units);
+      status = launch_k(kern, grid, kGatherThreads, c.smem, c.K, st, data, d3, (U)m, (U)n, (U)c.W, (U)c.SB,
+                        (U)c.max_slots, n_strips, (U)c.H, (int)c.halo, off, F, G, stw);
     }
-    go(OffAffine<U, false>{FastDiv<U>((uint64_t)m)}, MapId<U>{}, PermR2CPre<U>(m, cc, binv));
-  } else {  // form 3, p = {a, c, m, q}
-    const int64_t cc = f.p[1] > 0 ? f.p[1] : 1, a = f.p[0] > 0 ? f.p[0] : 1;
-    const int64_t q = ((f.p[3] % a) + a) % a;
-    go(OffAffine<U, true>{FastDiv<U>((uint64_t)m)}, PermR2CPre<U>(m, cc, q), MapId<U>{});
-  }
+  };
+  with_local_maps<U>(f, m, go);
   return status;
 }
 
@@ -651,7 +758,20 @@ int launch_col_gather(const FnSpec &f, char *data, int64_t d3, int64_t m, int64_
                       cudaStream_t st, LaunchStats *ls) {
   if (m <= 0 || n <= 0 || d3 <= 0) return T213_OK;
   const LocalCfg lc = local_col_config(f, m, n, eb, data);
-  if (lc.ok) {
+  if (lc.ok && lc.peel) {
+    int status = T213_ERR_UNSUPPORTED;
+    if (eb == 4)
+      status = lc.u64 ? launch_col_peel_t<4, uint64_t>(f, lc, data, d3, m, n, st)
+                      : launch_col_peel_t<4, uint32_t>(f, lc, data, d3, m, n, st);
+    else if (eb == 8)
+      status = lc.u64 ? launch_col_peel_t<8, uint64_t>(f, lc, data, d3, m, n, st)
+                      : launch_col_peel_t<8, uint32_t>(f, lc, data, d3, m, n, st);
+    if (status != kNoCluster) {
+      if (ls) ls->launches++;
+      return status;
+    }
+  }
+  if (lc.ok && !lc.peel) {
     int status = T213_ERR_UNSUPPORTED;
     auto run = [&](auto EBc, auto AWc) -> bool {
       constexpr int EB = decltype(EBc)::value;

@@ -210,7 +210,7 @@ int t213_tune_shape(void *scratch_data, int64_t d1, int64_t d2, int64_t d3, int3
       int8_t Variant::*field;
       std::vector<int8_t> values;
     };
-    const Knob knobs[] = {{PT_COL, &Variant::col, {1, 2, 3, 4}},
+    const Knob knobs[] = {{PT_COL, &Variant::col, {1, 2, 3, 4, 5}},
                           {PT_ROW, &Variant::row, {2, 3}},
                           {PT_TILE, &Variant::tile, {1, 2}},
                           {PT_SEG, &Variant::seg, {2, 3}}};

@@ -86,9 +86,12 @@ CONFIG_PLANS = [
 @pytest.mark.parametrize("shape", [(7919, 6151, 2, 8), (8192, 6143, 2, 4), (6151, 7919, 2, 8)])
 def test_tall_column_passes_use_the_cluster_local_kernel(t213, shape):
     """Coprime configurations take the cluster-local column gather with
-    128-byte strips."""
+    128-byte strips split over a cluster."""
+    import re
     desc = t213.describe(*shape)
-    assert "[local W=" in desc and "cluster=8" in desc, desc
+    m = re.search(r"\[local W=(\d+) cluster=(\d+)", desc)
+    assert m, desc
+    assert int(m.group(1)) * shape[3] == 128 and int(m.group(2)) >= 2, desc
 
 
 @pytest.mark.parametrize("shape,prefix", CONFIG_PLANS, ids=lambda v: str(v))
@@ -118,3 +121,15 @@ def test_launch_counts(t213):
     assert t213.plan_launches(1024, 1024, 1, 16) == 1
     assert t213.plan_launches(8192, 6144, 4, 4) in (2, 3)
     assert t213.plan_launches(7919, 6151, 2, 8) == 2
+
+
+def test_describe_names_the_peeled_column_kernel(t213):
+    """Column passes over a pitch that is not a 16-byte multiple take the
+    peeled cluster-local kernel for 4- and 8-byte elements; a 16-byte pitch
+    keeps the plain one."""
+    d = t213.describe(7919, 6151, 2, 8, "c2r")
+    assert "[local W=16 cluster" in d and "peeled]" in d, d
+    d = t213.describe(7919, 601, 1, 4, "r2c")
+    assert "col_gather(fn=22)[local W=32" in d and "aw=16 peeled]" in d, d
+    d = t213.describe(8192, 6143, 2, 4, "c2r")
+    assert "col_gather(fn=21)[local W=32 cluster" in d and "peeled" not in d, d
