@@ -97,3 +97,40 @@ def test_batch_full_config_round_trip(cuda, t213):
     assert back.status() == 0
     bad = [shapes[i] for i in range(512) if not cuda.equal(devs[i], origs[i])]
     assert not bad, bad[:5]
+
+
+def test_batch_unaligned_column_items(cuda, oracle, t213):
+    """Column items over pitches that are not 16-byte multiples (4- and
+    8-byte elements, word-width accesses): tensors of odd and 2 mod 4 row
+    lengths, column heights up to about 1200, placed in one buffer at bases
+    off a 16-byte boundary with guard bytes between them.  Each tensor must
+    match the oracle and no guard byte may change."""
+    specs = [(701, 333, 1, 4, "c2r"), (333, 701, 2, 4, "r2c"), (1001, 1187, 1, 8, "c2r"), (1187, 1001, 1, 8, "r2c"),
+             (998, 601, 2, 4, "c2r"), (601, 998, 1, 4, "r2c"), (97, 1201, 3, 8, "c2r"), (1201, 97, 3, 8, "r2c"),
+             (35, 35, 4, 8, "c2r"), (5, 3, 7, 4, "r2c"), (4001, 9, 2, 4, "c2r"), (9, 4001, 2, 8, "r2c")]
+    guard = 64
+    offs, pos = [], guard
+    for i, (d1, d2, d3, eb, _) in enumerate(specs):
+        pos += (4 * (i % 3 + 1)) if eb == 4 else 8  # bases 4, 8 or 12 past a 16-byte boundary
+        offs.append(pos)
+        pos += d1 * d2 * d3 * eb + guard
+        pos = (pos + 15) // 16 * 16
+    host = np.full(pos, 0xC3, np.uint8)
+    wants = []
+    for i, ((d1, d2, d3, eb, _), o) in enumerate(zip(specs, offs)):
+        x = oracle.random_bits(d1 * d2 * d3, eb, 500 + i)
+        host[o:o + x.nbytes] = x.view(np.uint8)
+        wants.append(oracle.gather213(x.view(np.dtype((np.void, eb))), d1, d2, d3).view(np.uint8))
+    dev = to_device(cuda, host)
+    views = [dev[o:o + d1 * d2 * d3 * eb] for (d1, d2, d3, eb, _), o in zip(specs, offs)]
+    B = t213.Batch([(v, d1, d2, d3, eb, plan) for v, (d1, d2, d3, eb, plan) in zip(views, specs)])
+    B.execute()
+    assert B.status() == 0
+    got = from_device(dev)
+    mask = np.ones(pos, bool)
+    for (d1, d2, d3, eb, plan), o, want in zip(specs, offs, wants):
+        n = d1 * d2 * d3 * eb
+        assert np.array_equal(got[o:o + n], want), (d1, d2, d3, eb, plan, o)
+        mask[o:o + n] = False
+    assert (got[mask] == 0xC3).all(), "bytes outside the tensors were written"
+    B.close()
