@@ -442,6 +442,19 @@ struct OffAffine {
 
 constexpr int kColHaloMax = 64;  // largest halo (dmax - dmin) a strip may need
 
+// The barrier between a strip's loads and its stores in the cluster-local
+// column kernels.  Each thread has waited for its own cp.async copies, so
+// every global read of the strip has been performed and its value sits in
+// shared memory: the cluster barrier only has to order execution (no CTA
+// stores before every CTA's reads are done), and a relaxed arrive spares each
+// thread the release fence, which would wait for its previous strip's global
+// stores to drain.  The CTA barrier before it makes the staged shared memory
+// visible to all threads of the CTA.
+__device__ __forceinline__ void strip_loaded_barrier() {
+  __syncthreads();
+  asm volatile("barrier.cluster.arrive.relaxed.aligned;\n\tbarrier.cluster.wait.aligned;" ::: "memory");
+}
+
 template <int EB, int AW, typename U, typename Off, typename Fsrc, typename Gout, bool CLUSTER>
 __global__ void __launch_bounds__(kGatherThreads)
     k_col_local(char *__restrict__ data, int64_t d3, U m, U n, U W, U WS, int64_t n_strips, U H, int halo, Off off,
@@ -555,7 +568,7 @@ __global__ void __launch_bounds__(kGatherThreads)
       if constexpr (AW >= 4) cp_async_wait_all();
       // every CTA of the strip has read its rows before anyone writes
       if (CLUSTER)
-        cg::this_cluster().sync();
+        strip_loaded_barrier();
       else
         __syncthreads();
       for (U ob = (U)warp * 32; ob < nout; ob += (U)nwarps * 32) {
@@ -587,7 +600,7 @@ __global__ void __launch_bounds__(kGatherThreads)
       }
       if constexpr (AW >= 4) cp_async_wait_all();
       if (CLUSTER)
-        cg::this_cluster().sync();
+        strip_loaded_barrier();
       else
         __syncthreads();
       const uint32_t nwo = (uint32_t)nout * wpr;
@@ -734,7 +747,7 @@ __global__ void __launch_bounds__(kGatherThreads)
       }
       cp_async_wait_all();
       if (CLUSTER)
-        cg::this_cluster().sync();
+        strip_loaded_barrier();
       else
         __syncthreads();
       // ---- stores: the shifts of the 2 PER - 1 columns a lane may take -----
@@ -794,7 +807,7 @@ __global__ void __launch_bounds__(kGatherThreads)
       }
       cp_async_wait_all();
       if (CLUSTER)
-        cg::this_cluster().sync();
+        strip_loaded_barrier();
       else
         __syncthreads();
       const uint32_t nwo = (uint32_t)nout * (uint32_t)wn;
