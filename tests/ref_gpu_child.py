@@ -7,7 +7,9 @@ reference prefetches its argument as managed memory, src/transpose.cu:104),
 calls ``inplace::transpose<T>`` of the reference's library compiled from its
 sources (``oracle/_ref/libref_inplace.so``, through ``oracle/ref_gpu_shim.cu``)
 and writes a digest of the result bytes, and for small jobs the bytes
-themselves, to the result file.
+themselves, to the result file.  A job with ``time_reps`` also times that
+many further calls on the resident buffer (wall time per call, best and
+median; each call ends in a device synchronisation).
 
 The reference runs here and not inside pytest because it prints to stdout and
 exits the process on a CUDA error (src/cudacheck.cu:4-9); in a child process
@@ -22,6 +24,7 @@ import hashlib
 import json
 import os
 import sys
+import time
 
 import numpy as np
 
@@ -83,8 +86,19 @@ def main() -> int:
         rc = L.ref_inplace_transpose_typed(p, d1, d2, d3, code)
         y = np.empty_like(x)
         ctypes.memmove(y.ctypes.data, p, nbytes)
-        L.ref_free_managed(p)
         res = {"rc": int(rc), "digest": digest(y)}
+        if rc == 0 and job.get("time_reps"):
+            # timing of further calls on the resident (already prefetched)
+            # buffer; each call ends in cudaDeviceSynchronize, so the wall
+            # time of a call is its launches, kernels and host work
+            ts = []
+            for _ in range(int(job["time_reps"])):
+                t0 = time.perf_counter()
+                L.ref_inplace_transpose_typed(p, d1, d2, d3, code)
+                ts.append((time.perf_counter() - t0) * 1e3)
+            ts.sort()
+            res["ms_best"], res["ms_median"] = round(ts[0], 4), round(ts[len(ts) // 2], 4)
+        L.ref_free_managed(p)
         if job.get("save"):
             y.tofile(job["save"])
         results[job["name"]] = res
