@@ -668,7 +668,7 @@ __global__ void __launch_bounds__(kGatherThreads)
   const int64_t pitch = (int64_t)n * EB;
   const uint32_t pm = (uint32_t)(pitch & 15);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const uint32_t L = (uint32_t)(W * EB / 16);  // lanes per row; divides 32 (host: W * EB in {64, 128, 256})
+  const uint32_t L = (uint32_t)(W * EB / 16);  // lanes per row; divides 32 (host: W * EB in {64, 128, 256, 512})
   const uint32_t rpi = 32 / L, lr = lane / L, lw = lane - lr * L;
 
   for (int64_t u = unit0; u < n_units; u += ustride) {
